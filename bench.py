@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the hist training path on the 10M x 100 binary workload.
+
+A step is one boosting round (gradients, row sampling, one depth-8 tree,
+margin update) over all 10M rows of the synthetic `binary_mixed` dataset
+(70 N(0,1), 20 lognormal, 10 Bernoulli(0.05) features, 10% NaN;
+binary:logistic, max_depth 8, max_bin 256, eta 0.05, subsample 0.8,
+colsample_bytree 0.8), with the fixed-point histogram form by default.
+
+  value : Mrow-rounds/s with the binned matrix resident in HBM (CUDA events
+          on the library's stream, max over ranks).
+  e2e   : the same metric through the public C ABI call sb_train() from
+          pinned host buffers: upload, cuts + binning, K rounds, model
+          download.
+  roofline : the histogram kernel (dominant), algorithmic bytes / device time.
+  cpu_baseline : the C++ restatement of the reference CPU hist path, all
+          host threads, on a bounded row sample, rounds only.
+
+`--impl reference` times the reference's CPU path (the oracle port: the Rust
+reference cannot be built here) with all host threads on a bounded sample of
+the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "train Mrow-rounds/s at matched RMSE; serving predict p50/p99 ms vs plain GPU"
+UNIT = "Mrow-rounds/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=10_000_000)
+    ap.add_argument("--precision", default="fixed", choices=["fixed", "fp32"])
+    ap.add_argument("--cpu-rows", type=int, default=250_000)
+    ap.add_argument("--cpu-rounds", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--seed", type=int, default=1)
+    return ap.parse_args()
+
+
+def params_for(sb, precision):
+    return sb.TrainingParams(objective="binary:logistic", max_depth=8, max_bin=256, eta=0.05,
+                             subsample=0.8, colsample_bytree=0.8, hist_precision=precision, seed=7)
+
+
+def config_of(args, n):
+    return {"workload": f"binary_mixed {n} x 100 (binary:logistic, depth 8, max_bin 256, eta 0.05, "
+                        "subsample 0.8, colsample_bytree 0.8)",
+            "n_rows": n, "n_features": 100, "rounds_per_step": 1, "precision": args.precision,
+            "l2": "inputs larger than L2 (ELLPACK 2 B/entry = 2.1 GB at 10M rows)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.tmp,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.06)
+        self.proc.terminate()
+        self.proc.wait()
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """dram read+write bytes of one histogram launch, from the committed ncu
+    summary of the same kernel (scaled to this workload), or None."""
+    path = os.path.join(ROOT, "profiles", "k_hist_traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d
+    except (OSError, ValueError):
+        return None
+
+
+def logloss(margin, y):
+    p = 1.0 / (1.0 + np.exp(-margin.astype(np.float64)))
+    p = np.clip(p, 1e-15, 1 - 1e-15)
+    return float(np.mean(-(y * np.log(p) + (1 - y) * np.log(1 - p))))
+
+
+def cpu_leg(x, y, args, sb, threads, rounds, rows):
+    import __graft_entry__ as ge
+    orc = ge._load_module("sb_pyoracle", os.path.join(ROOT, "oracle", "pyoracle.py")).Oracle()
+    xs = np.ascontiguousarray(x[:rows])
+    ys = np.ascontiguousarray(y[:rows])
+    p = params_for(sb, "fp32")
+    t0 = time.perf_counter()
+    d = orc.data(xs, max_bin=256)
+    t_bin = time.perf_counter() - t0
+    times = []
+    for _ in range(rounds):
+        t0 = time.perf_counter()
+        orc.train(xs, ys, p, 1, threads=threads, data=d)
+        times.append(time.perf_counter() - t0)
+    return xs.shape[0], times, t_bin
+
+
+def run_reference(args):
+    """The reference arm: the reference's CPU hist path (oracle port), all host
+    threads, a bounded sample of the same workload per step."""
+    import __graft_entry__ as ge
+    sb = ge.load_package()
+    from sequoia_boost_b200 import datagen
+    threads = os.cpu_count() or 1
+    rows = args.cpu_rows
+    x, y = datagen.binary_mixed(n=rows, seed=args.seed, chunk=min(rows, 500_000))
+    orc = ge._load_module("sb_pyoracle", os.path.join(ROOT, "oracle", "pyoracle.py")).Oracle()
+    d = orc.data(x, max_bin=256)
+    p = params_for(sb, "fp32")
+    for _ in range(args.warmup):
+        orc.train(x, y, p, 1, threads=threads, data=d)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.train(x, y, p, 1, threads=threads, data=d)
+    t = time.perf_counter() - t0
+    value = rows * args.steps / t / 1e6
+    cfg = config_of(args, args.rows)
+    cfg["sample_rows"] = rows
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"first {rows} rows of binary_mixed, one round per step "
+                                       "(binning excluded); the Rust reference cannot be built here"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    sb = ge.load_package()
+    from sequoia_boost_b200 import datagen
+    ctx = sb.Context(local)
+    n = args.rows
+    x, y = datagen.binary_mixed(n=n, seed=args.seed + rank)
+    p = params_for(sb, args.precision)
+    xd = torch.from_numpy(x).to(f"cuda:{local}")
+    gh = sb.GHistIndex.from_device(xd.data_ptr(), n, x.shape[1], max_bin=256, ctx=ctx)
+    del xd
+    torch.cuda.synchronize()
+    b = sb.Booster(gh, p, y, ctx=ctx)
+    for _ in range(args.warmup):
+        b.update(1)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = ctx.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.update(1)
+    e1.record(stream)
+    launches = ctx.launch_count() - l0
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * n * args.steps / (ms / 1e3) / 1e6
+
+    # roofline of the histogram kernel: algorithmic bytes / device time
+    b.set_timing(True)
+    b.reset_stats()
+    b.update(min(args.steps, 5))
+    st = b.stats()
+    b.set_timing(False)
+    peak, peak_kind = peaks()
+    achieved = st["hist_bytes"] / (st["hist_ms"] / 1e3) / 1e9 if st["hist_ms"] > 0 else None
+    tr = traffic_per_launch()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": None if achieved is None else achieved / peak, "peak_kind": peak_kind,
+                "traffic": None if tr is None else tr.get("bytes_per_launch"),
+                "kernel": f"k_hist<{'fixed' if args.precision == 'fixed' else 'fp32'}>",
+                "launches_timed": st["hist_launches"],
+                "bytes_per_launch": st["hist_bytes"] / max(st["hist_launches"], 1),
+                "ms_per_launch": st["hist_ms"] / max(st["hist_launches"], 1),
+                "hist_share_of_round": st["hist_ms"] / st["round_ms"] if st["round_ms"] else None}
+    quality = {"train_logloss_after_rounds": logloss(b.margins().reshape(-1), y),
+               "rounds": args.warmup + args.steps + min(args.steps, 5),
+               "quant_err_grad": st["quant_err_grad"], "quant_err_hess": st["quant_err_hess"]}
+    del b
+    del gh
+
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        xp = torch.from_numpy(x).pin_memory()
+        yp = torch.from_numpy(y).pin_memory()
+        xh = xp.numpy()
+        yh = yp.numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = sb.train(p, sb.DMatrix(xh, labels=yh), args.steps, ctx=ctx)
+        t1 = time.perf_counter()
+        off, nodes, coff, cats, w = m.export()
+        d2h = nodes.nbytes + off.nbytes + coff.nbytes + cats.nbytes
+        e2e = {"value": n * args.steps / (t1 - t0) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": (xh.nbytes + yh.nbytes) / args.steps,
+               "d2h_bytes_per_step": d2h / args.steps,
+               "note": "one sb_train() call from pinned host X/y: upload, cuts+binning, "
+                       f"{args.steps} rounds, model download; bytes amortised per round"}
+        del m, xp, yp
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        rows, times, t_bin = cpu_leg(x, y, args, sb, threads, args.cpu_rounds, args.cpu_rows)
+        cpu = {"value": rows * len(times) / sum(times) / 1e6, "unit": UNIT, "cores": threads,
+               "kind": "port",
+               "sample": f"first {rows} rows, {len(times)} rounds, binning excluded "
+                         f"(binning {t_bin:.1f} s single-threaded)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "i64" if args.precision == "fixed" else "f32", "data": "synthetic",
+                "config": config_of(args, n), "clocks": clk, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "quality": quality}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

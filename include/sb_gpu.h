@@ -1,0 +1,295 @@
+/*
+ * sb_gpu.h — C ABI of sequoia-boost-b200: the B200 (sm_100a) backend for
+ * sequoia-boost's `tree_method=hist` training and tree-ensemble prediction.
+ *
+ * Every entry point below stands in for one interface of the reference crate
+ * (pgarrett-scripps/sequoia-boost, crates/sequoia-boost/src/…); each cites the
+ * file:line it replaces. Plain pointers and sizes only: no CUDA or torch types
+ * cross the boundary (device pointers are passed as `void*`/typed pointers
+ * where an entry says "device").
+ *
+ * Conventions
+ *  - Every function returns an `int` status: SB_OK (0) or one of SB_ERR_*;
+ *    `sb_last_error()` gives a thread-local message for the last failure.
+ *    Nothing exits, aborts or traps. (The reference's HistogramBackend is
+ *    infallible and panics on misuse, tree/hist/mod.rs:31-45; its crate API
+ *    returns Result<_, SequoiaError>, error.rs:6-76.)
+ *  - Host buffers are borrowed for the duration of a call and never retained.
+ *  - Device memory belongs to opaque handles (sb_ctx, sb_ghist, sb_booster,
+ *    sb_model) and is released by the matching *_destroy.
+ *  - One CUDA stream per sb_ctx; a context is not re-entrant (the caller
+ *    serialises calls on it); distinct contexts are independent.
+ *  - There is no CPU fallback: without a usable sm_100 device every compute
+ *    entry returns SB_ERR_NO_DEVICE.
+ */
+#ifndef SB_GPU_H
+#define SB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  SB_OK = 0,
+  SB_ERR_INVALID_ARG = 1,  /* SequoiaError::InvalidParameter */
+  SB_ERR_OOM = 2,          /* device allocation failed */
+  SB_ERR_CUDA = 3,         /* any other CUDA runtime error */
+  SB_ERR_TIMEOUT = 4,      /* a bounded device wait gave up */
+  SB_ERR_UNSUPPORTED = 5,  /* valid for the reference, not built here */
+  SB_ERR_NO_DEVICE = 6,    /* no CUDA device / wrong architecture */
+  SB_ERR_DIMENSION = 7     /* SequoiaError::DimensionMismatch */
+};
+
+/* Thread-local text of the last error (never NULL). */
+const char* sb_last_error(void);
+/* Library version string. */
+const char* sb_version(void);
+
+/* ----------------------------------------------------------------- types */
+/* GradPair{grad:f32, hess:f32} — objective/mod.rs:31-36 (8 bytes). */
+typedef struct sb_gradpair { float grad; float hess; } sb_gradpair;
+/* GradStats{grad:f64, hess:f64} — tree/gain.rs:18-23 (16 bytes). */
+typedef struct sb_gradstats { double grad; double hess; } sb_gradstats;
+
+/* Node — tree/regtree.rs:17-47. left/right are -1 for a leaf; for a
+ * categorical node categories[cat_begin..cat_end) of the owning tree are the
+ * category codes routed left. 40 bytes. */
+typedef struct sb_node {
+  int32_t left;
+  int32_t right;
+  uint32_t split_feature;
+  float split_cond;
+  float leaf_value;
+  float sum_hess;
+  float split_gain;
+  uint8_t default_left;
+  uint8_t is_categorical;
+  uint16_t reserved;
+  uint32_t cat_begin;
+  uint32_t cat_end;
+} sb_node;
+
+enum { SB_FEAT_NUMERICAL = 0, SB_FEAT_CATEGORICAL = 1 }; /* data/meta.rs:8-14 */
+
+enum { /* create_objective, objective/mod.rs:136-161 */
+  SB_OBJ_SQUARED_ERROR = 0, /* reg:squarederror | reg:linear */
+  SB_OBJ_PSEUDOHUBER = 1,   /* reg:pseudohubererror */
+  SB_OBJ_LOGISTIC = 2,      /* binary:logistic | reg:logistic */
+  SB_OBJ_SOFTMAX = 3,       /* multi:softmax */
+  SB_OBJ_SOFTPROB = 4       /* multi:softprob */
+};
+
+enum { SB_GROW_DEPTHWISE = 0, SB_GROW_LOSSGUIDE = 1 }; /* config GrowPolicy */
+
+enum { /* histogram accumulation on the device */
+  SB_HIST_FP32 = 0,  /* f32 shared-memory partials, f64 node histograms */
+  SB_HIST_FIXED = 1  /* per-round power-of-two int quantised gradients,
+                        exact int64 histograms (order independent) */
+};
+
+/* TrainingParams fields on the hist path — config/params.rs:76-151, defaults
+ * :153-186. 8-byte fields first so the layout has no interior padding. */
+typedef struct sb_train_params {
+  uint64_t seed;              /* 0 */
+  double base_score;          /* used when has_base_score != 0 */
+  double eta;                 /* 0.3 */
+  double gamma;               /* 0 */
+  double min_child_weight;    /* 1 */
+  double max_delta_step;      /* 0 */
+  double subsample;           /* 1 */
+  double colsample_bytree;    /* 1 */
+  double colsample_bylevel;   /* 1 */
+  double colsample_bynode;    /* 1 */
+  double lambda;              /* 1 */
+  double alpha;               /* 0 */
+  double scale_pos_weight;    /* 1 */
+  const int8_t* monotone;     /* n_monotone entries of -1/0/+1, or NULL */
+  const uint32_t* interaction_offsets;  /* n_interaction_groups + 1 */
+  const uint32_t* interaction_features; /* flattened groups */
+  int32_t objective;          /* SB_OBJ_* */
+  int32_t num_class;          /* 0 */
+  int32_t has_base_score;     /* 0 = estimate from labels */
+  int32_t max_depth;          /* 6 (0 = unlimited) */
+  int32_t max_leaves;         /* 0 */
+  int32_t grow_policy;        /* SB_GROW_* */
+  int32_t max_bin;            /* 256 */
+  int32_t hist_precision;     /* SB_HIST_* */
+  int32_t quantize_bits;      /* fixed-point magnitude bits, 0 = 16 */
+  int32_t n_monotone;
+  int32_t n_interaction_groups;
+  int32_t reserved;
+} sb_train_params;
+
+/* Fills `p` with the reference defaults (params.rs:153-186). */
+void sb_train_params_default(sb_train_params* p);
+/* TrainingParams::validate, params.rs:197-261, plus the limits of this
+ * backend. SB_OK or SB_ERR_INVALID_ARG / SB_ERR_UNSUPPORTED. */
+int sb_train_params_validate(const sb_train_params* p);
+
+/* A read-only view of a tree ensemble (BoostedModel, learner/model.rs:34-54).
+ * Tree t owns nodes[tree_node_offset[t] .. tree_node_offset[t+1]) and
+ * categories[tree_cat_offset[t] .. tree_cat_offset[t+1]). */
+typedef struct sb_model_view {
+  const int64_t* tree_node_offset;  /* n_trees + 1 */
+  const sb_node* nodes;
+  const int64_t* tree_cat_offset;   /* n_trees + 1 */
+  const uint32_t* categories;
+  const float* tree_weights;        /* n_trees, or NULL for all 1.0 */
+  int32_t n_trees;
+  int32_t num_class;                /* 0/1 = single output */
+  int32_t n_features;
+  int32_t objective;                /* SB_OBJ_* for pred_transform */
+  float base_score;                 /* margin space */
+  int32_t reserved;
+} sb_model_view;
+
+/* --------------------------------------------------------------- context */
+typedef struct sb_ctx sb_ctx;
+
+/* Opens device `device` (must be sm_100) with its own stream. */
+int sb_ctx_create(int device, sb_ctx** out);
+int sb_ctx_destroy(sb_ctx* ctx);
+int sb_ctx_synchronize(sb_ctx* ctx);
+/* The context's cudaStream_t, for event timing by the caller. */
+void* sb_ctx_stream(sb_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+uint64_t sb_ctx_launch_count(const sb_ctx* ctx);
+
+/* ------------------------------------------- binned matrix (cuts + ELLPACK)
+ * Replaces HistCuts::from_dmatrix (data/quantile.rs:39-70, with
+ * build_feature_cuts :203-245, build_categorical_cuts :187-200,
+ * push_max_sentinel :319-323) and GHistIndex::from_dmatrix (data/ghist.rs:
+ * :48-82, bin_of quantile.rs:166-181). `X` is a dense row-major f32 matrix;
+ * an entry is missing when it is NaN (missing = NaN) or equal to `missing`
+ * (data/dmatrix.rs:10-16). `feature_types` may be NULL (all numerical).
+ * The device keeps local bins per feature as u16, 0xFFFF = missing. */
+typedef struct sb_ghist sb_ghist;
+
+int sb_ghist_create(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
+                    const uint8_t* feature_types, float missing, int max_bin,
+                    sb_ghist** out);
+/* Same from a device-resident matrix `d_X` (n_rows * n_cols floats). */
+int sb_ghist_create_device(sb_ctx* ctx, const float* d_X, size_t n_rows, size_t n_cols,
+                           const uint8_t* feature_types, float missing, int max_bin,
+                           sb_ghist** out);
+int sb_ghist_destroy(sb_ghist* g);
+int sb_ghist_info(const sb_ghist* g, size_t* n_rows, size_t* n_cols, size_t* total_bins);
+/* HistCuts accessors (quantile.rs:126-163): feature_offset[n_cols+1],
+ * cut_values[total_bins], is_categorical[n_cols]. Any pointer may be NULL. */
+int sb_ghist_cuts(const sb_ghist* g, uint32_t* feature_offset, float* cut_values,
+                  uint8_t* is_categorical);
+/* Local bin of every entry, row-major n_rows * n_cols, 0xFFFF = missing. The
+ * reference's global bin is feature_offset[f] + local (ghist.rs:48-82). */
+int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins);
+
+/* -------------------------------------------- HistogramBackend (the seam)
+ * trait HistogramBackend::build, tree/hist/mod.rs:31-45 / CpuBackend::build
+ * :58-89: out[bin] = sum over rows r and r's bins of (grad_r, hess_r), f64,
+ * overwritten, length total_bins. `precision` is SB_HIST_*; with
+ * SB_HIST_FIXED the pairs are first quantised with the power-of-two scale of
+ * this call's max |grad| / |hess| over the `n` pairs. */
+int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m,
+                  const sb_gradpair* gpair, size_t n, int precision, int quantize_bits,
+                  sb_gradstats* out, size_t total_bins);
+/* HistogramBackend::subtract, hist/mod.rs:38-44 (and `subtracted` :25-28). */
+int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats* child,
+                     sb_gradstats* out, size_t total_bins);
+
+/* ---------------------------------------------------- tree / boosting loop */
+typedef struct sb_model sb_model;
+typedef struct sb_booster sb_booster;
+
+/* HistTreeBuilder::build, tree/builder/hist.rs:139-202: one tree from the
+ * binned matrix, `gpair[n]`, and the row subset `rows[m]` (ascending).
+ * Column sampling is that of class `k` in round `round` (sb_sampling.h).
+ * Leaves are NOT scaled by eta (the builder's contract). `row_leaf`, when not
+ * NULL, receives for every row of the subset the node id it ends in (the
+ * row-to-node assignment; -1 for rows outside the subset, length n). */
+int sb_tree_build(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p,
+                  const sb_gradpair* gpair, size_t n, const uint32_t* rows, size_t m,
+                  uint64_t round, uint32_t k, int32_t* row_leaf, sb_model** out);
+
+/* The device-resident boosting state of train_impl (learner/train.rs:183-383)
+ * for the hist path: labels/weights/margins live on the device; each update
+ * runs whole rounds (gradients, row sampling, one tree per output, margin
+ * update) without host round trips. `base_margin` is NULL or n (or n*K)
+ * floats (init_margin, train.rs:496-511). Host pointers. */
+int sb_booster_create(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p,
+                      const float* labels, const float* weights, const float* base_margin,
+                      sb_booster** out);
+/* Runs `n_rounds` boosting rounds (the unit of work of one training step). */
+int sb_booster_update(sb_booster* b, int n_rounds);
+/* Margins [n][K] (host). */
+int sb_booster_margins(const sb_booster* b, float* out);
+/* Gradient pairs of the last round, class-major [K][n] (host). */
+int sb_booster_gradients(const sb_booster* b, sb_gradpair* out);
+/* Rows sampled in round `round` (host, n bytes: 1 = in the subset). */
+int sb_booster_row_mask(const sb_booster* b, uint64_t round, uint8_t* out);
+/* Copies the trees grown so far into a new model handle. */
+int sb_booster_model(const sb_booster* b, sb_model** out);
+int sb_booster_destroy(sb_booster* b);
+
+typedef struct sb_booster_stats {
+  uint64_t rounds;             /* rounds completed */
+  uint64_t hist_launches;      /* histogram-kernel launches (timed ones) */
+  double hist_ms;              /* summed device time of those launches */
+  double hist_bytes;           /* algorithmic bytes they processed */
+  double round_ms;             /* summed device time of timed rounds */
+  double quant_err_grad;       /* last round: max |g - deq(q(g))| */
+  double quant_err_hess;       /* last round: max |h - deq(q(h))| */
+  int32_t quant_shift_grad;    /* last round's power-of-two scale exponents */
+  int32_t quant_shift_hess;
+} sb_booster_stats;
+/* timing != 0 brackets every histogram launch with CUDA events (adds a
+ * little overhead); stats accumulate until reset. */
+int sb_booster_set_timing(sb_booster* b, int timing);
+int sb_booster_stats_get(const sb_booster* b, sb_booster_stats* out);
+int sb_booster_stats_reset(sb_booster* b);
+
+/* train(params, dtrain, num_boost_round), learner/train.rs:107-113 (hist
+ * branch): the whole job from host buffers — upload, cuts and binning,
+ * `num_boost_round` rounds, model download. */
+int sb_train(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
+             const uint8_t* feature_types, float missing, const float* labels,
+             const float* weights, const float* base_margin, const sb_train_params* p,
+             int num_boost_round, sb_model** out);
+
+/* ------------------------------------------------------ model / predict */
+/* Uploads a host ensemble (BoostedModel) to the device. */
+int sb_model_create(sb_ctx* ctx, const sb_model_view* view, sb_model** out);
+int sb_model_destroy(sb_model* m);
+/* Sizes of the host export arrays. */
+int sb_model_export_sizes(const sb_model* m, int32_t* n_trees, int64_t* n_nodes,
+                          int64_t* n_categories);
+/* Host export: tree_node_offset[n_trees+1], nodes[n_nodes],
+ * tree_cat_offset[n_trees+1], categories[n_categories], tree_weights[n_trees].
+ * Any pointer may be NULL. base_score / num_class / n_features / objective
+ * via sb_model_info. */
+int sb_model_export(const sb_model* m, int64_t* tree_node_offset, sb_node* nodes,
+                    int64_t* tree_cat_offset, uint32_t* categories, float* tree_weights);
+int sb_model_info(const sb_model* m, float* base_score, int32_t* num_class,
+                  int32_t* n_features, int32_t* objective);
+
+/* BoostedModel::predict_margin_limited, learner/model.rs:231-285: f32 sum in
+ * tree order, tree t adds w_t * leaf to output t % K; `ntree_limit` 0 = all.
+ * `base_margin` NULL or n / n*K floats. Host X [n][n_cols], out [n][K]. */
+int sb_predict_margin(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
+                      float missing, const float* base_margin, size_t ntree_limit,
+                      float* out);
+/* BoostedModel::predict, model.rs:291-300 (margin then pred_transform). */
+int sb_predict(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float missing,
+               const float* base_margin, float* out);
+/* BoostedModel::predict_contribs, learner/shap.rs:321-367: out
+ * [n][K][n_cols+1], bias last. */
+int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
+                        float missing, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SB_GPU_H */

@@ -1,0 +1,35 @@
+"""sequoia-boost-b200: the B200 backend of sequoia-boost's hist training path.
+
+A thin Python mirror of the reference crate's public API (crates/sequoia-boost/
+src/lib.rs:86-97) over the C ABI in include/sb_gpu.h:
+
+    TrainingParams   config/params.rs:76-373
+    DMatrix          data/dmatrix.rs (dense f32 storage)
+    train            learner/train.rs:107-113
+    BoostedModel     learner/model.rs (predict_margin, predict, predict_contribs)
+    GHistIndex       data/ghist.rs + data/quantile.rs (device-resident cuts/bins)
+    GpuBackend       tree/hist/mod.rs:31-45 (HistogramBackend: build, subtract)
+    HistTreeBuilder  tree/builder/hist.rs:98-202
+    Booster          the device-resident state of train_impl's round loop
+
+All compute runs in libsb_gpu.so on an sm_100 GPU; there is no CPU fallback.
+"""
+from .api import (  # noqa: F401
+    BoostedModel,
+    Booster,
+    Context,
+    DMatrix,
+    GHistIndex,
+    GpuBackend,
+    HistTreeBuilder,
+    Monotone,
+    TrainingParams,
+    default_context,
+    train,
+)
+from ._abi import SbError  # noqa: F401
+
+__all__ = [
+    "BoostedModel", "Booster", "Context", "DMatrix", "GHistIndex", "GpuBackend",
+    "HistTreeBuilder", "Monotone", "SbError", "TrainingParams", "default_context", "train",
+]

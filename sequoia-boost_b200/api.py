@@ -1,0 +1,574 @@
+"""Python mirror of the reference crate's API over libsb_gpu.so (see __init__)."""
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _abi as A
+
+OBJECTIVES = {
+    "reg:squarederror": A.SB_OBJ_SQUARED_ERROR,
+    "reg:linear": A.SB_OBJ_SQUARED_ERROR,
+    "reg:pseudohubererror": A.SB_OBJ_PSEUDOHUBER,
+    "binary:logistic": A.SB_OBJ_LOGISTIC,
+    "reg:logistic": A.SB_OBJ_LOGISTIC,
+    "multi:softmax": A.SB_OBJ_SOFTMAX,
+    "multi:softprob": A.SB_OBJ_SOFTPROB,
+}
+
+
+class Monotone:
+    """config/params.rs:60-68."""
+    NONE = 0
+    INCREASING = 1
+    DECREASING = -1
+
+
+@dataclass
+class TrainingParams:
+    """TrainingParams with the reference's field names and defaults
+    (config/params.rs:76-186). `hist_precision` ("fp32" | "fixed") and
+    `quantize_bits` select this backend's histogram form."""
+    seed: int = 0
+    objective: str = "reg:squarederror"
+    num_class: int = 0
+    base_score: Optional[float] = None
+    eta: float = 0.3
+    gamma: float = 0.0
+    max_depth: int = 6
+    max_leaves: int = 0
+    min_child_weight: float = 1.0
+    max_delta_step: float = 0.0
+    subsample: float = 1.0
+    colsample_bytree: float = 1.0
+    colsample_bylevel: float = 1.0
+    colsample_bynode: float = 1.0
+    lambda_: float = 1.0
+    alpha: float = 0.0
+    scale_pos_weight: float = 1.0
+    grow_policy: str = "depthwise"
+    max_bin: int = 256
+    monotone_constraints: List[int] = field(default_factory=list)
+    interaction_constraints: List[List[int]] = field(default_factory=list)
+    hist_precision: str = "fp32"
+    quantize_bits: int = 0
+
+    @staticmethod
+    def builder():
+        return _ParamsBuilder()
+
+    def to_c(self):
+        """A C struct plus the buffers it points into (keep both alive)."""
+        p = A.SbTrainParams()
+        A.lib().sb_train_params_default(ctypes.byref(p))
+        if self.objective not in OBJECTIVES:
+            raise A.SbError(A.SB_ERR_INVALID_ARG, f"unknown value `{self.objective}` for objective")
+        p.seed = self.seed
+        p.objective = OBJECTIVES[self.objective]
+        p.num_class = self.num_class
+        p.has_base_score = 0 if self.base_score is None else 1
+        p.base_score = 0.0 if self.base_score is None else float(self.base_score)
+        p.eta = self.eta
+        p.gamma = self.gamma
+        p.max_depth = self.max_depth
+        p.max_leaves = self.max_leaves
+        p.min_child_weight = self.min_child_weight
+        p.max_delta_step = self.max_delta_step
+        p.subsample = self.subsample
+        p.colsample_bytree = self.colsample_bytree
+        p.colsample_bylevel = self.colsample_bylevel
+        p.colsample_bynode = self.colsample_bynode
+        p.lambda_ = self.lambda_
+        p.alpha = self.alpha
+        p.scale_pos_weight = self.scale_pos_weight
+        p.grow_policy = A.SB_GROW_LOSSGUIDE if self.grow_policy == "lossguide" else A.SB_GROW_DEPTHWISE
+        p.max_bin = self.max_bin
+        p.hist_precision = A.SB_HIST_FIXED if self.hist_precision == "fixed" else A.SB_HIST_FP32
+        p.quantize_bits = self.quantize_bits
+        keep = []
+        if self.monotone_constraints:
+            mono = np.asarray(self.monotone_constraints, dtype=np.int8)
+            keep.append(mono)
+            p.monotone = A.ptr(mono, ctypes.c_int8)
+            p.n_monotone = len(mono)
+        if self.interaction_constraints:
+            offs = [0]
+            flat = []
+            for g in self.interaction_constraints:
+                flat += list(g)
+                offs.append(len(flat))
+            o = np.asarray(offs, dtype=np.uint32)
+            fl = np.asarray(flat if flat else [0], dtype=np.uint32)
+            keep += [o, fl]
+            p.interaction_offsets = A.ptr(o, ctypes.c_uint32)
+            p.interaction_features = A.ptr(fl, ctypes.c_uint32)
+            p.n_interaction_groups = len(self.interaction_constraints)
+        return p, keep
+
+    def validate(self):
+        p, _keep = self.to_c()
+        A.check(A.lib().sb_train_params_validate(ctypes.byref(p)))
+        return self
+
+
+class _ParamsBuilder:
+    """TrainingParamsBuilder (params.rs:264-373): chained setters."""
+
+    def __init__(self):
+        self.params = TrainingParams()
+
+    def __getattr__(self, name):
+        key = "lambda_" if name in ("lambda_", "reg_lambda") else name
+
+        def setter(value):
+            setattr(self.params, key, value)
+            return self
+        return setter
+
+    def build(self):
+        return self.params.validate()
+
+    def build_unchecked(self):
+        return self.params
+
+
+class Context:
+    """A device context (sb_ctx): one GPU, one CUDA stream."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_ctx_create(device, ctypes.byref(h)))
+        self.h = h
+
+    def synchronize(self):
+        A.check(A.lib().sb_ctx_synchronize(self.h))
+
+    def stream(self):
+        return A.lib().sb_ctx_stream(self.h)
+
+    def launch_count(self):
+        return A.lib().sb_ctx_launch_count(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            A.lib().sb_ctx_destroy(self.h)
+            self.h = None
+
+
+_DEFAULT = None
+
+
+def default_context():
+    global _DEFAULT
+    if _DEFAULT is None:
+        _DEFAULT = Context(0)
+    return _DEFAULT
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class DMatrix:
+    """A dense f32 dataset with labels/weights/base margin (data/dmatrix.rs).
+    Missing entries are NaN, or equal to `missing` (dmatrix.rs:10-16)."""
+
+    def __init__(self, data, labels=None, weights=None, base_margin=None, feature_types=None,
+                 missing=float("nan")):
+        x = _f32(data)
+        if x.ndim != 2 or x.shape[0] == 0 or x.shape[1] == 0:
+            raise A.SbError(A.SB_ERR_INVALID_ARG, "empty dataset: from_dense: zero rows or columns")
+        self.data = x
+        self.missing = float(missing)
+        self.labels = None if labels is None else _f32(labels)
+        self.weights = None if weights is None else _f32(weights)
+        self.base_margin = None if base_margin is None else _f32(base_margin)
+        self.feature_types = feature_types
+        for name, v in (("labels", self.labels), ("weights", self.weights)):
+            if v is not None and v.shape[0] != x.shape[0]:
+                raise A.SbError(A.SB_ERR_DIMENSION, f"dimension mismatch: {name}")
+
+    @staticmethod
+    def from_dense(data, n_rows, n_cols, missing=float("nan")):
+        a = _f32(data)
+        if a.size != n_rows * n_cols:
+            raise A.SbError(A.SB_ERR_DIMENSION, "dimension mismatch: dense data length")
+        return DMatrix(a.reshape(n_rows, n_cols), missing=missing)
+
+    def with_labels(self, labels):
+        self.labels = _f32(labels)
+        return self
+
+    def with_weights(self, weights):
+        self.weights = _f32(weights)
+        return self
+
+    def with_base_margin(self, bm):
+        self.base_margin = _f32(bm)
+        return self
+
+    def with_feature_types(self, types):
+        self.feature_types = list(types)
+        return self
+
+    @property
+    def n_rows(self):
+        return self.data.shape[0]
+
+    @property
+    def n_cols(self):
+        return self.data.shape[1]
+
+    def _ftypes(self):
+        if self.feature_types is None:
+            return None
+        return np.asarray([1 if t in (1, "c", "categorical") else 0 for t in self.feature_types],
+                          dtype=np.uint8)
+
+
+class GHistIndex:
+    """HistCuts + GHistIndex resident on the device (sb_ghist)."""
+
+    def __init__(self, dmat: DMatrix, max_bin=256, ctx: Context = None, device_ptr=None):
+        self.ctx = ctx or default_context()
+        h = ctypes.c_void_p()
+        ft = dmat._ftypes() if dmat is not None else None
+        A.check(A.lib().sb_ghist_create(self.ctx.h, A.ptr(dmat.data, ctypes.c_float), dmat.n_rows,
+                                        dmat.n_cols, A.ptr(ft, ctypes.c_uint8), dmat.missing, max_bin,
+                                        ctypes.byref(h)))
+        self.h = h
+        self._keep = ft
+
+    @classmethod
+    def from_device(cls, d_ptr, n_rows, n_cols, max_bin=256, missing=float("nan"), feature_types=None,
+                    ctx: Context = None):
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        ft = None if feature_types is None else np.asarray(feature_types, dtype=np.uint8)
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_ghist_create_device(self.ctx.h, ctypes.c_void_p(d_ptr), n_rows, n_cols,
+                                               A.ptr(ft, ctypes.c_uint8), missing, max_bin,
+                                               ctypes.byref(h)))
+        self.h = h
+        self._keep = ft
+        return self
+
+    def info(self):
+        n, f, t = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        A.check(A.lib().sb_ghist_info(self.h, ctypes.byref(n), ctypes.byref(f), ctypes.byref(t)))
+        return n.value, f.value, t.value
+
+    @property
+    def total_bins(self):
+        return self.info()[2]
+
+    def cuts(self):
+        """(feature_offset[F+1], cut_values[total_bins], is_categorical[F])."""
+        n, f, t = self.info()
+        off = np.zeros(f + 1, np.uint32)
+        vals = np.zeros(t, np.float32)
+        cat = np.zeros(f, np.uint8)
+        A.check(A.lib().sb_ghist_cuts(self.h, A.ptr(off, ctypes.c_uint32), A.ptr(vals, ctypes.c_float),
+                                      A.ptr(cat, ctypes.c_uint8)))
+        return off, vals, cat
+
+    def local_bins(self):
+        n, f, _ = self.info()
+        out = np.zeros((n, f), np.uint16)
+        A.check(A.lib().sb_ghist_bins(self.h, A.ptr(out, ctypes.c_uint16)))
+        return out
+
+    def global_bins(self):
+        """Global bin per entry (feature_offset[f] + local), UINT32_MAX = missing."""
+        off, _, _ = self.cuts()
+        lb = self.local_bins().astype(np.uint32)
+        g = lb + off[:-1][None, :]
+        g[lb == 0xFFFF] = 0xFFFFFFFF
+        return g
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            A.lib().sb_ghist_destroy(self.h)
+            self.h = None
+
+
+def _gpair(gpair):
+    g = np.ascontiguousarray(gpair, dtype=np.float32)
+    if g.ndim == 1:
+        g = g.reshape(-1, 2)
+    return np.ascontiguousarray(g)
+
+
+class GpuBackend:
+    """HistogramBackend on the device (tree/hist/mod.rs:31-45)."""
+
+    def __init__(self, precision="fp32", quantize_bits=0, ctx: Context = None):
+        self.precision = A.SB_HIST_FIXED if precision == "fixed" else A.SB_HIST_FP32
+        self.bits = quantize_bits
+        self.ctx = ctx or default_context()
+
+    def build(self, ghist: GHistIndex, rows, gpair, out=None):
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        g = _gpair(gpair)
+        total = ghist.total_bins
+        if out is None:
+            out = np.zeros((total, 2), np.float64)
+        A.check(A.lib().sb_hist_build(self.ctx.h, ghist.h, A.ptr(rows, ctypes.c_uint32), rows.size,
+                                      g.ctypes.data_as(ctypes.POINTER(A.SbGradPair)), g.shape[0],
+                                      self.precision, self.bits,
+                                      out.ctypes.data_as(ctypes.POINTER(A.SbGradStats)), total))
+        return out
+
+    def subtract(self, parent, child, out=None):
+        p = np.ascontiguousarray(parent, dtype=np.float64)
+        c = np.ascontiguousarray(child, dtype=np.float64)
+        if out is None:
+            out = np.zeros_like(p)
+        A.check(A.lib().sb_hist_subtract(self.ctx.h, p.ctypes.data_as(ctypes.POINTER(A.SbGradStats)),
+                                         c.ctypes.data_as(ctypes.POINTER(A.SbGradStats)),
+                                         out.ctypes.data_as(ctypes.POINTER(A.SbGradStats)),
+                                         p.shape[0]))
+        return out
+
+
+NODE_DTYPE = np.dtype([
+    ("left", "<i4"), ("right", "<i4"), ("split_feature", "<u4"), ("split_cond", "<f4"),
+    ("leaf_value", "<f4"), ("sum_hess", "<f4"), ("split_gain", "<f4"), ("default_left", "u1"),
+    ("is_categorical", "u1"), ("reserved", "<u2"), ("cat_begin", "<u4"), ("cat_end", "<u4")])
+assert NODE_DTYPE.itemsize == ctypes.sizeof(A.SbNode)
+
+
+class RegTree:
+    """A host copy of one tree (tree/regtree.rs:74-83)."""
+
+    def __init__(self, nodes, categories):
+        self.nodes = nodes
+        self.categories = categories
+
+    def num_nodes(self):
+        return len(self.nodes)
+
+    def num_leaves(self):
+        return int((self.nodes["left"] == -1).sum())
+
+
+class BoostedModel:
+    """The trained ensemble (learner/model.rs:34-54); arrays live on the host,
+    a device copy is made on the first prediction."""
+
+    def __init__(self, handle, ctx: Context):
+        self.h = handle
+        self.ctx = ctx
+
+    @classmethod
+    def from_arrays(cls, node_off, nodes, cat_off, cats, base_score, num_class, n_features,
+                    objective="reg:squarederror", weights=None, ctx: Context = None):
+        ctx = ctx or default_context()
+        node_off = np.ascontiguousarray(node_off, np.int64)
+        nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+        cat_off = np.ascontiguousarray(cat_off, np.int64)
+        cats = np.ascontiguousarray(cats if len(cats) else np.zeros(1, np.uint32), np.uint32)
+        v = A.SbModelView()
+        v.tree_node_offset = A.ptr(node_off, ctypes.c_int64)
+        v.nodes = nodes.ctypes.data_as(ctypes.POINTER(A.SbNode))
+        v.tree_cat_offset = A.ptr(cat_off, ctypes.c_int64)
+        v.categories = A.ptr(cats, ctypes.c_uint32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        v.tree_weights = A.ptr(w, ctypes.c_float)
+        v.n_trees = len(node_off) - 1
+        v.num_class = num_class
+        v.n_features = n_features
+        v.objective = OBJECTIVES.get(objective, objective) if isinstance(objective, str) else objective
+        v.base_score = base_score
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_model_create(ctx.h, ctypes.byref(v), ctypes.byref(h)))
+        return cls(h, ctx)
+
+    def export(self):
+        """(node_off, nodes, cat_off, cats, weights)."""
+        nt, nn, nc = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        A.check(A.lib().sb_model_export_sizes(self.h, ctypes.byref(nt), ctypes.byref(nn),
+                                              ctypes.byref(nc)))
+        node_off = np.zeros(nt.value + 1, np.int64)
+        nodes = np.zeros(nn.value, NODE_DTYPE)
+        cat_off = np.zeros(nt.value + 1, np.int64)
+        cats = np.zeros(max(nc.value, 1), np.uint32)
+        w = np.zeros(max(nt.value, 1), np.float32)
+        A.check(A.lib().sb_model_export(self.h, A.ptr(node_off, ctypes.c_int64),
+                                        nodes.ctypes.data_as(ctypes.POINTER(A.SbNode)),
+                                        A.ptr(cat_off, ctypes.c_int64), A.ptr(cats, ctypes.c_uint32),
+                                        A.ptr(w, ctypes.c_float)))
+        return node_off, nodes, cat_off, cats[:nc.value], w[:nt.value]
+
+    def info(self):
+        bs, k, f, o = ctypes.c_float(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        A.check(A.lib().sb_model_info(self.h, ctypes.byref(bs), ctypes.byref(k), ctypes.byref(f),
+                                      ctypes.byref(o)))
+        return bs.value, k.value, f.value, o.value
+
+    def base_score(self):
+        return self.info()[0]
+
+    def n_outputs(self):
+        k = self.info()[1]
+        return k if k >= 2 else 1
+
+    def num_trees(self):
+        return len(self.export()[0]) - 1
+
+    def trees(self):
+        off, nodes, coff, cats, _ = self.export()
+        return [RegTree(nodes[off[t]:off[t + 1]], cats[coff[t]:coff[t + 1]])
+                for t in range(len(off) - 1)]
+
+    def predict_margin_limited(self, d: DMatrix, ntree_limit=0):
+        k = self.n_outputs()
+        out = np.zeros((d.n_rows, k), np.float32)
+        bm = None
+        if d.base_margin is not None:
+            bm = d.base_margin
+            if bm.size == d.n_rows and k > 1:
+                bm = np.repeat(bm.reshape(-1, 1), k, axis=1)
+            bm = np.ascontiguousarray(bm.reshape(-1), np.float32)
+        A.check(A.lib().sb_predict_margin(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols,
+                                          d.missing, A.ptr(bm, ctypes.c_float), ntree_limit,
+                                          A.ptr(out, ctypes.c_float)))
+        return out.reshape(-1)
+
+    def predict_margin(self, d: DMatrix):
+        return self.predict_margin_limited(d, 0)
+
+    def predict(self, d: DMatrix):
+        k = self.n_outputs()
+        out = np.zeros((d.n_rows, k), np.float32)
+        bm = None
+        if d.base_margin is not None:
+            bm = np.ascontiguousarray(np.broadcast_to(d.base_margin.reshape(d.n_rows, -1),
+                                                      (d.n_rows, k)).reshape(-1), np.float32)
+        A.check(A.lib().sb_predict(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols, d.missing,
+                                   A.ptr(bm, ctypes.c_float), A.ptr(out, ctypes.c_float)))
+        return out.reshape(-1)
+
+    def predict_contribs(self, d: DMatrix):
+        k = self.n_outputs()
+        out = np.zeros((d.n_rows, k, d.n_cols + 1), np.float32)
+        A.check(A.lib().sb_predict_contribs(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols,
+                                            d.missing, A.ptr(out, ctypes.c_float)))
+        return out.reshape(-1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            A.lib().sb_model_destroy(self.h)
+            self.h = None
+
+
+def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Context = None):
+    """learner/train.rs:107-113 (hist branch): upload, cuts, binning, rounds,
+    model download — one C ABI call (sb_train)."""
+    ctx = ctx or default_context()
+    if dtrain.labels is None:
+        raise A.SbError(A.SB_ERR_INVALID_ARG, "empty dataset: train: dtrain has no labels")
+    p, keep = params.to_c()
+    ft = dtrain._ftypes()
+    bm = None
+    k = params.num_class if params.objective.startswith("multi:") else 1
+    if dtrain.base_margin is not None:
+        bm = dtrain.base_margin
+        if bm.size == dtrain.n_rows and k > 1:
+            bm = np.repeat(bm.reshape(-1, 1), k, axis=1)
+        bm = np.ascontiguousarray(bm.reshape(-1), np.float32)
+    h = ctypes.c_void_p()
+    A.check(A.lib().sb_train(ctx.h, A.ptr(dtrain.data, ctypes.c_float), dtrain.n_rows, dtrain.n_cols,
+                             A.ptr(ft, ctypes.c_uint8), dtrain.missing,
+                             A.ptr(dtrain.labels, ctypes.c_float), A.ptr(dtrain.weights, ctypes.c_float),
+                             A.ptr(bm, ctypes.c_float), ctypes.byref(p), num_boost_round,
+                             ctypes.byref(h)))
+    del keep
+    return BoostedModel(h, ctx)
+
+
+class HistTreeBuilder:
+    """HistTreeBuilder::build (tree/builder/hist.rs:139-202) on the device."""
+
+    def __init__(self, params: TrainingParams, ctx: Context = None):
+        self.params = params
+        self.ctx = ctx or default_context()
+
+    def build(self, ghist: GHistIndex, gpair, row_subset, round=0, k=0, return_row_leaf=False):
+        p, keep = self.params.to_c()
+        g = _gpair(gpair)
+        rows = np.ascontiguousarray(row_subset, np.uint32)
+        n = g.shape[0]
+        leaf = np.zeros(n, np.int32) if return_row_leaf else None
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_tree_build(self.ctx.h, ghist.h, ctypes.byref(p),
+                                      g.ctypes.data_as(ctypes.POINTER(A.SbGradPair)), n,
+                                      A.ptr(rows, ctypes.c_uint32), rows.size, round, k,
+                                      A.ptr(leaf, ctypes.c_int32), ctypes.byref(h)))
+        del keep
+        m = BoostedModel(h, self.ctx)
+        return (m, leaf) if return_row_leaf else m
+
+
+class Booster:
+    """The device-resident round loop (sb_booster): labels, margins,
+    gradients and row lists stay on the GPU; `update(r)` runs r rounds."""
+
+    def __init__(self, ghist: GHistIndex, params: TrainingParams, labels, weights=None,
+                 base_margin=None, ctx: Context = None):
+        self.ctx = ctx or ghist.ctx
+        self.ghist = ghist
+        self.params = params
+        p, keep = params.to_c()
+        lab = _f32(labels)
+        w = None if weights is None else _f32(weights)
+        bm = None if base_margin is None else _f32(base_margin)
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_booster_create(self.ctx.h, ghist.h, ctypes.byref(p),
+                                          A.ptr(lab, ctypes.c_float), A.ptr(w, ctypes.c_float),
+                                          A.ptr(bm, ctypes.c_float), ctypes.byref(h)))
+        del keep
+        self.h = h
+        self.n = lab.shape[0]
+        self.k = params.num_class if params.objective.startswith("multi:") else 1
+
+    def update(self, rounds=1):
+        A.check(A.lib().sb_booster_update(self.h, rounds))
+
+    def margins(self):
+        out = np.zeros((self.n, self.k), np.float32)
+        A.check(A.lib().sb_booster_margins(self.h, A.ptr(out, ctypes.c_float)))
+        return out
+
+    def gradients(self):
+        out = np.zeros((self.k, self.n, 2), np.float32)
+        A.check(A.lib().sb_booster_gradients(self.h, out.ctypes.data_as(ctypes.POINTER(A.SbGradPair))))
+        return out
+
+    def row_mask(self, round_):
+        out = np.zeros(self.n, np.uint8)
+        A.check(A.lib().sb_booster_row_mask(self.h, round_, A.ptr(out, ctypes.c_uint8)))
+        return out.astype(bool)
+
+    def model(self):
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_booster_model(self.h, ctypes.byref(h)))
+        return BoostedModel(h, self.ctx)
+
+    def set_timing(self, on=True):
+        A.check(A.lib().sb_booster_set_timing(self.h, 1 if on else 0))
+
+    def stats(self):
+        s = A.SbBoosterStats()
+        A.check(A.lib().sb_booster_stats_get(self.h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in A.SbBoosterStats._fields_}
+
+    def reset_stats(self):
+        A.check(A.lib().sb_booster_stats_reset(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            A.lib().sb_booster_destroy(self.h)
+            self.h = None

@@ -1,0 +1,57 @@
+"""In-tree build of libsb_gpu.so (sm_100a) with nvcc.
+
+Every CUDA source is compiled for `sm_100a` only, with `-fmad=false` so that
+no multiply-add is contracted: the FP64 split scan and the f32 leaf / margin
+arithmetic then round exactly as the CPU oracle (and the reference) round.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libsb_gpu.so")
+SOURCES = ["sb_core.cu", "sb_bin.cu", "sb_hist.cu", "sb_grow.cu", "sb_predict.cu"]
+HEADERS = ["sb_internal.cuh"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = [
+    "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+    "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+    "-Xptxas", "-warn-spills",
+]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose=False, extra_flags=()):
+    os.makedirs(BUILD, exist_ok=True)
+    inc = [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(HERE, "..", "include", "sb_gpu.h"),
+        os.path.join(HERE, "..", "include", "sb_sampling.h")]
+    objs = []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if _newer(o, [s] + inc):
+            cmd = [NVCC, *FLAGS, *extra_flags, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if _newer(LIB, objs):
+        cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
+               "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, extra_flags=sys.argv[1:])

@@ -1,0 +1,417 @@
+// sb_hist.cu — gradient histogram construction (K4) and subtraction (K5).
+//
+// Replaces CpuBackend::build / accumulate (tree/hist/mod.rs:58-119) and
+// `subtracted` / HistogramBackend::subtract (:25-28, :38-44).
+//
+// Design: a persistent grid (one or more CTAs per SM) splits the concatenated
+// rows of every node to build (all frontier nodes of all class trees in one
+// launch) evenly over CTAs. A CTA keeps one node's histogram for one feature
+// tile in shared memory, walks the node's row list with one warp per row and
+// one lane per feature (coalesced 64-byte reads of the row's u16 bins), adds
+// into shared memory, and flushes non-zero bins to the node's HBM histogram
+// with global atomics when it moves to the next node.
+//   FP32 form : two f32 shared atomics per entry; HBM histograms in f64.
+//   FIXED form: gradients pre-rounded to |q| <= 2^bits with a per-round
+//               power-of-two scale and packed as (q_g << 32) + q_h; one 64-bit
+//               integer shared atomic per entry accumulates both halves
+//               exactly (carries cannot cross: sum q_h < 2^32 and
+//               |sum q_g| < 2^31 are kept by flushing every
+//               fixed_rows_per_flush(bits) rows); HBM histograms in int64.
+// Each feature also owns one extra "missing" bin (index total_bins + f), so a
+// node's missing-value statistics are summed directly instead of being
+// recovered as total - present.
+#include "sb_internal.cuh"
+
+namespace sb {
+namespace {
+
+constexpr int HIST_THREADS = 1024;
+constexpr int MAX_TILE_FEATURES = 128;  // 4 features per lane
+constexpr int ROWS_PER_WARP = 4;        // rows in flight per warp
+
+struct HistDev {
+  const uint16_t* bins;
+  const uint32_t* foff;
+  size_t Fp;
+  size_t n;              // gradient column stride
+  int total_bins;
+  const void* gpair;
+  const HistItem* items;
+  const uint64_t* prefix;
+  const int* count;
+  const FeatureTile* tiles;
+  int ntiles;
+  uint32_t flush_rows;   // FIXED: max rows per shared partial
+  unsigned long long* rows_done;  // sampled rows accumulated (or null)
+};
+
+__device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
+  int lo = 0, hi = count;  // last i with prefix[i] <= pos
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= pos) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <bool FIXED>
+__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
+  extern __shared__ unsigned long long sh_u64[];
+  float* sh_f = reinterpret_cast<float*>(sh_u64);
+  __shared__ double s_tot_d[2];
+  __shared__ unsigned long long s_tot_u;
+
+  const int count = *a.count;
+  if (count <= 0) return;
+  const uint64_t W = a.prefix[count];
+  if (W == 0) return;
+  const uint64_t U = W * (uint64_t)a.ntiles;
+  const uint64_t lo = U * blockIdx.x / gridDim.x, hi = U * (blockIdx.x + 1) / gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+  uint64_t u = lo;
+  while (u < hi) {
+    const int t = (int)(u / W);
+    const uint64_t pos = u - (uint64_t)t * W;
+    const int it = find_item(a.prefix, count, pos);
+    const HistItem item = a.items[it];
+    const uint64_t item_lo = a.prefix[it], item_hi = a.prefix[it + 1];
+    uint64_t piece_hi_u = (uint64_t)t * W + item_hi;
+    if (piece_hi_u > hi) piece_hi_u = hi;
+    uint64_t n_pos = piece_hi_u - u;
+    if (FIXED && n_pos > a.flush_rows) n_pos = a.flush_rows;
+    const uint32_t pbeg = item.begin + (uint32_t)(pos - item_lo);
+    const uint32_t pend = pbeg + (uint32_t)n_pos;
+    const FeatureTile tile = a.tiles[t];
+    const int nf = tile.f1 - tile.f0;
+    const int nent = tile.nbins + nf;
+    const bool want_total = item.root && t == 0;
+
+    // per-lane features of this tile
+    int lbase[4], lmiss[4], lf[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int fl = lane + 32 * j;
+      lf[j] = fl < nf ? tile.f0 + fl : -1;
+      lbase[j] = lf[j] >= 0 ? (int)a.foff[lf[j]] - tile.bin0 : 0;
+      lmiss[j] = tile.nbins + fl;
+    }
+    for (int i = threadIdx.x; i < nent; i += blockDim.x) sh_u64[i] = 0ull;
+    if (threadIdx.x == 0) {
+      s_tot_d[0] = 0.0;
+      s_tot_d[1] = 0.0;
+      s_tot_u = 0ull;
+    }
+    __syncthreads();
+
+    double tg = 0.0, th = 0.0;
+    unsigned long long tq = 0ull;
+    unsigned int nsampled = 0;
+    const size_t gcol = (size_t)item.k * a.n;
+    for (uint32_t p = pbeg + warp * ROWS_PER_WARP; p < pend; p += nwarps * ROWS_PER_WARP) {
+      uint32_t rid[ROWS_PER_WARP];
+#pragma unroll
+      for (int q = 0; q < ROWS_PER_WARP; ++q) {
+        uint32_t pp = p + q;
+        rid[q] = pp < pend ? item.rows[pp] : UNSAMPLED;
+      }
+      float gg[ROWS_PER_WARP], hh[ROWS_PER_WARP];
+      unsigned long long pk[ROWS_PER_WARP];
+      uint16_t bv[ROWS_PER_WARP][4];
+#pragma unroll
+      for (int q = 0; q < ROWS_PER_WARP; ++q) {
+        const bool use = !(rid[q] & UNSAMPLED);
+        const size_t id = rid[q] & ~UNSAMPLED;
+        if (FIXED) {
+          pk[q] = use ? reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + id] : 0ull;
+        } else {
+          float2 v = use ? reinterpret_cast<const float2*>(a.gpair)[gcol + id] : make_float2(0.f, 0.f);
+          gg[q] = v.x;
+          hh[q] = v.y;
+        }
+        const uint16_t* brow = a.bins + id * a.Fp;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bv[q][j] = (use && lf[j] >= 0) ? __ldg(brow + lf[j]) : (uint16_t)0xFFFEu;
+      }
+#pragma unroll
+      for (int q = 0; q < ROWS_PER_WARP; ++q) {
+        if (rid[q] & UNSAMPLED) continue;
+        nsampled++;
+        if (want_total && lane == 0) {
+          if (FIXED) tq += pk[q];
+          else {
+            tg += (double)gg[q];
+            th += (double)hh[q];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint16_t b = bv[q][j];
+          if (b == 0xFFFEu) continue;
+          const int idx = (b == MISSING_BIN) ? lmiss[j] : lbase[j] + b;
+          if (FIXED) {
+            atomicAdd(&sh_u64[idx], pk[q]);
+          } else {
+            atomicAdd(&sh_f[2 * idx], gg[q]);
+            atomicAdd(&sh_f[2 * idx + 1], hh[q]);
+          }
+        }
+      }
+    }
+    if (a.rows_done && lane == 0 && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
+    if (want_total && lane == 0) {
+      if (FIXED) atomicAdd(&s_tot_u, tq);
+      else {
+        atomicAdd(&s_tot_d[0], tg);
+        atomicAdd(&s_tot_d[1], th);
+      }
+    }
+    __syncthreads();
+    // flush the partial into the node's HBM histogram
+    for (int i = threadIdx.x; i < nent; i += blockDim.x) {
+      const int gi = i < tile.nbins ? tile.bin0 + i : a.total_bins + tile.f0 + (i - tile.nbins);
+      if (FIXED) {
+        unsigned long long v = sh_u64[i];
+        if (v) {
+          unsigned long long hq = v & 0xFFFFFFFFull;
+          long long gq = ((long long)(v - hq)) >> 32;
+          unsigned long long* o = reinterpret_cast<unsigned long long*>(item.out) + 2 * (size_t)gi;
+          if (gq) atomicAdd(o, (unsigned long long)gq);
+          if (hq) atomicAdd(o + 1, hq);
+        }
+      } else {
+        float g = sh_f[2 * i], h = sh_f[2 * i + 1];
+        double* o = reinterpret_cast<double*>(item.out) + 2 * (size_t)gi;
+        if (g != 0.0f) atomicAdd(o, (double)g);
+        if (h != 0.0f) atomicAdd(o + 1, (double)h);
+      }
+    }
+    if (want_total && threadIdx.x == 0) {
+      if (FIXED) {
+        unsigned long long v = s_tot_u;
+        unsigned long long hq = v & 0xFFFFFFFFull;
+        long long gq = ((long long)(v - hq)) >> 32;
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(item.total);
+        atomicAdd(o, (unsigned long long)gq);
+        atomicAdd(o + 1, hq);
+      } else {
+        double* o = reinterpret_cast<double*>(item.total);
+        atomicAdd(o, s_tot_d[0]);
+        atomicAdd(o + 1, s_tot_d[1]);
+      }
+    }
+    __syncthreads();
+    u += n_pos;
+  }
+}
+
+__global__ void k_zero_items(const HistItem* __restrict__ items, const int* __restrict__ count,
+                             size_t words) {
+  int it = blockIdx.y;
+  if (it >= *count) return;
+  unsigned long long* o = reinterpret_cast<unsigned long long*>(items[it].out);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+       i += (size_t)gridDim.x * blockDim.x)
+    o[i] = 0ull;
+  if (items[it].root && blockIdx.x == 0 && threadIdx.x < 2)
+    reinterpret_cast<unsigned long long*>(items[it].total)[threadIdx.x] = 0ull;
+}
+
+__global__ void k_subtract(const double2* __restrict__ p, const double2* __restrict__ c,
+                           double2* __restrict__ o, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double2 a = p[i], b = c[i];
+    o[i] = make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+  }
+}
+
+__global__ void k_fixed_to_f64(const longlong2* __restrict__ in, double2* __restrict__ out, size_t n,
+                               double sg, double sh) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    longlong2 v = in[i];
+    out[i] = make_double2(__dmul_rn((double)v.x, sg), __dmul_rn((double)v.y, sh));
+  }
+}
+
+}  // namespace
+
+int hist_prepare(sb_ctx* ctx, Ghist* g) {
+  size_t budget = ctx->smem_optin > 8192 ? ctx->smem_optin - 4096 : ctx->smem_optin;
+  g->tiles.clear();
+  size_t F = g->F, f0 = 0, maxb = 0;
+  while (f0 < F) {
+    size_t f1 = f0;
+    while (f1 < F && f1 - f0 < (size_t)MAX_TILE_FEATURES) {
+      size_t bins = g->h_foff[f1 + 1] - g->h_foff[f0];
+      if ((bins + (f1 + 1 - f0)) * 8 > budget) break;
+      f1++;
+    }
+    SB_REQUIRE(f1 > f0, SB_ERR_UNSUPPORTED, "feature %zu has too many bins for shared memory", f0);
+    FeatureTile t;
+    t.f0 = (int)f0;
+    t.f1 = (int)f1;
+    t.bin0 = (int)g->h_foff[f0];
+    t.nbins = (int)(g->h_foff[f1] - g->h_foff[f0]);
+    maxb = std::max(maxb, (size_t)(t.nbins + (t.f1 - t.f0)) * 8);
+    g->tiles.push_back(t);
+    f0 = f1;
+  }
+  g->hist_smem_bytes = maxb;
+  SB_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));
+  SB_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));
+  return SB_OK;
+}
+
+int hist_grid(sb_ctx* ctx, const Ghist* g) {
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist<true>, HIST_THREADS,
+                                                g->hist_smem_bytes);
+  if (per_sm < 1) per_sm = 1;
+  return ctx->num_sms * per_sm;
+}
+
+int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
+  HistDev a;
+  a.bins = L.g->bins.p;
+  a.foff = L.g->foff.p;
+  a.Fp = L.g->Fp;
+  a.n = L.g->n;
+  a.total_bins = (int)L.g->total_bins;
+  a.gpair = L.gpair;
+  a.items = L.items;
+  a.prefix = L.prefix;
+  a.count = L.count;
+  a.tiles = L.tiles;
+  a.ntiles = L.ntiles;
+  a.flush_rows = fixed_rows_per_flush(L.quant_bits);
+  a.rows_done = L.rows_done;
+  int grid = hist_grid(ctx, L.g);
+  if (L.fixed) SB_LAUNCH(ctx, k_hist<true>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
+  else SB_LAUNCH(ctx, k_hist<false>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
+  return SB_OK;
+}
+
+int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const int* count,
+                      int max_items) {
+  if (max_items <= 0) return SB_OK;
+  size_t words = (g->total_bins + g->F) * 2;
+  dim3 grid((unsigned)std::min<size_t>((words + 255) / 256, 64), (unsigned)max_items);
+  SB_LAUNCH(ctx, k_zero_items, grid, 256, 0, items, count, words);
+  return SB_OK;
+}
+
+// per-node seam helpers (defined in sb_grow.cu)
+int quantize_pairs(sb_ctx* ctx, const float2* d_gp, size_t n, int bits, unsigned long long* d_packed,
+                   int* h_shift_g, int* h_shift_h);
+
+}  // namespace sb
+
+extern "C" {
+
+int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m,
+                  const sb_gradpair* gpair, size_t n, int precision, int quantize_bits,
+                  sb_gradstats* out, size_t total_bins) {
+  using namespace sb;
+  SB_REQUIRE(ctx && g && gpair && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(m == 0 || rows, SB_ERR_INVALID_ARG, "rows is NULL");
+  SB_REQUIRE(total_bins == g->total_bins, SB_ERR_DIMENSION,
+             "dimension mismatch: out length expected %zu, got %zu", g->total_bins, total_bins);
+  SB_REQUIRE(n == g->n, SB_ERR_DIMENSION, "dimension mismatch: gpair length expected %zu, got %zu",
+             g->n, n);
+  SB_REQUIRE(precision == SB_HIST_FP32 || precision == SB_HIST_FIXED, SB_ERR_INVALID_ARG,
+             "unknown precision %d", precision);
+  int bits = quantize_bits ? quantize_bits : 16;
+  SB_REQUIRE(bits >= 8 && bits <= 23, SB_ERR_INVALID_ARG, "quantize_bits must be in [8, 23]");
+  for (size_t i = 0; i < m; ++i)
+    SB_REQUIRE(rows[i] < n, SB_ERR_INVALID_ARG, "row %u out of range", rows[i]);
+  SB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t HB = g->total_bins + g->F;
+  DBuf<uint32_t> d_rows;
+  DBuf<float2> d_gp;
+  DBuf<unsigned long long> d_packed;
+  DBuf<double2> d_hist, d_out;
+  DBuf<HistItem> d_item;
+  DBuf<uint64_t> d_prefix;
+  DBuf<int> d_count;
+  DBuf<FeatureTile> d_tiles;
+  SB_TRY(d_rows.alloc(ctx, std::max<size_t>(m, 1)));
+  SB_TRY(d_gp.alloc(ctx, n));
+  SB_TRY(d_hist.alloc(ctx, HB));
+  SB_TRY(d_out.alloc(ctx, HB));
+  SB_TRY(d_item.alloc(ctx, 1));
+  SB_TRY(d_prefix.alloc(ctx, 2));
+  SB_TRY(d_count.alloc(ctx, 1));
+  SB_TRY(d_tiles.alloc(ctx, g->tiles.size()));
+  if (m) SB_CUDA(cudaMemcpyAsync(d_rows.p, rows, m * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_gp.p, gpair, n * 8, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_tiles.p, g->tiles.data(), g->tiles.size() * sizeof(FeatureTile),
+                          cudaMemcpyHostToDevice, st));
+  int sg = 0, shh = 0;
+  const void* gsrc = d_gp.p;
+  if (precision == SB_HIST_FIXED) {
+    SB_TRY(d_packed.alloc(ctx, n));
+    SB_TRY(quantize_pairs(ctx, d_gp.p, n, bits, d_packed.p, &sg, &shh));
+    gsrc = d_packed.p;
+  }
+  HistItem it;
+  it.rows = d_rows.p;
+  it.begin = 0;
+  it.end = (uint32_t)m;
+  it.k = 0;
+  it.root = 0;
+  it.out = d_hist.p;
+  it.total = nullptr;
+  uint64_t prefix[2] = {0, (uint64_t)m};
+  int one = 1;
+  SB_CUDA(cudaMemcpyAsync(d_item.p, &it, sizeof(it), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_prefix.p, prefix, sizeof(prefix), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_count.p, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemsetAsync(d_hist.p, 0, d_hist.bytes(), st));
+  HistLaunch L;
+  L.g = g;
+  L.gpair = gsrc;
+  L.fixed = precision == SB_HIST_FIXED;
+  L.quant_bits = bits;
+  L.items = d_item.p;
+  L.prefix = d_prefix.p;
+  L.count = d_count.p;
+  L.max_items = 1;
+  L.tiles = d_tiles.p;
+  L.ntiles = (int)g->tiles.size();
+  L.rows_done = nullptr;
+  if (m) SB_TRY(launch_hist(ctx, L));
+  const double2* res = d_hist.p;
+  if (L.fixed) {
+    SB_LAUNCH(ctx, k_fixed_to_f64, 256, 256, 0, reinterpret_cast<const longlong2*>(d_hist.p), d_out.p,
+              HB, std::ldexp(1.0, -sg), std::ldexp(1.0, -shh));
+    res = d_out.p;
+  }
+  SB_CUDA(cudaMemcpyAsync(out, res, total_bins * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SB_OK;
+}
+
+int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats* child,
+                     sb_gradstats* out, size_t total_bins) {
+  using namespace sb;
+  SB_REQUIRE(ctx && parent && child && out, SB_ERR_INVALID_ARG, "NULL argument");
+  if (total_bins == 0) return SB_OK;
+  SB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  DBuf<double2> p, c, o;
+  SB_TRY(p.alloc(ctx, total_bins));
+  SB_TRY(c.alloc(ctx, total_bins));
+  SB_TRY(o.alloc(ctx, total_bins));
+  SB_CUDA(cudaMemcpyAsync(p.p, parent, p.bytes(), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(c.p, child, c.bytes(), cudaMemcpyHostToDevice, st));
+  unsigned blocks = (unsigned)std::min<size_t>((total_bins + 255) / 256, (size_t)ctx->num_sms * 8);
+  SB_LAUNCH(ctx, k_subtract, blocks, 256, 0, p.p, c.p, o.p, total_bins);
+  SB_CUDA(cudaMemcpyAsync(out, o.p, o.bytes(), cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SB_OK;
+}
+
+}  // extern "C"

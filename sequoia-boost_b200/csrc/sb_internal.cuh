@@ -1,0 +1,277 @@
+// sb_internal.cuh — shared declarations of the sequoia-boost-b200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/sb_gpu.h"
+#include "../../include/sb_sampling.h"
+
+namespace sb {
+
+void set_error(const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what, const char* file, int line);
+
+}  // namespace sb
+
+#define SB_CUDA(call)                                                      \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) return sb::cuda_status(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define SB_TRY(expr)              \
+  do {                            \
+    int s_ = (expr);              \
+    if (s_ != SB_OK) return s_;   \
+  } while (0)
+
+#define SB_REQUIRE(cond, code, ...)   \
+  do {                                \
+    if (!(cond)) {                    \
+      sb::set_error(__VA_ARGS__);     \
+      return (code);                  \
+    }                                 \
+  } while (0)
+
+// Launch on the context stream, count it, and surface launch errors.
+#define SB_LAUNCH(ctx, kern, grid, block, smem, ...)                        \
+  do {                                                                      \
+    kern<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);          \
+    (ctx)->launches++;                                                      \
+    SB_CUDA(cudaGetLastError());                                            \
+  } while (0)
+
+struct sb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  size_t smem_optin = 0;     // max dynamic shared memory per block
+  size_t smem_per_sm = 0;
+  uint64_t launches = 0;
+};
+
+namespace sb {
+
+// Stream-ordered device allocation (pool-backed, cached across calls).
+int dalloc(sb_ctx* ctx, void** p, size_t bytes);
+void dfree(sb_ctx* ctx, void* p);
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  sb_ctx* ctx = nullptr;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  int alloc(sb_ctx* c, size_t count) {
+    release();
+    ctx = c;
+    n = count;
+    if (count == 0) return SB_OK;
+    return dalloc(c, (void**)&p, count * sizeof(T));
+  }
+  void release() {
+    if (p && ctx) dfree(ctx, p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ----------------------------------------------------------------- data
+constexpr uint16_t MISSING_BIN = 0xFFFF;
+constexpr int MAX_CAT_BINS = 256;      // categorical features: <= 256 categories
+constexpr uint32_t UNSAMPLED = 0x80000000u;  // row-list flag: not in the subset
+
+// A feature tile of the histogram: features [f0, f1), whose bins fit in the
+// shared-memory partial of one CTA.
+struct FeatureTile {
+  int f0, f1;
+  int bin0;       // foff[f0]
+  int nbins;      // foff[f1] - foff[f0]
+};
+
+struct Ghist {  // sb_ghist
+  sb_ctx* ctx = nullptr;
+  size_t n = 0, F = 0, Fp = 0;   // Fp: padded row stride in u16
+  size_t total_bins = 0;
+  int max_bin = 0;
+  float missing = NAN;
+  int max_feature_bins = 0;
+  int has_categorical = 0;
+  DBuf<uint16_t> bins;     // [n][Fp] local bins
+  DBuf<uint32_t> foff;     // [F+1]
+  DBuf<float> cuts;        // [total_bins]
+  DBuf<uint8_t> is_cat;    // [F]
+  std::vector<uint32_t> h_foff;
+  std::vector<float> h_cuts;
+  std::vector<uint8_t> h_is_cat;
+  std::vector<FeatureTile> tiles;  // histogram feature tiles
+  size_t hist_smem_bytes = 0;      // max tile bytes (8 B per bin)
+};
+
+int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t* h_ftypes,
+                float missing, int max_bin, Ghist* g);
+
+// ------------------------------------------------------------ histograms
+// One node histogram to accumulate: rows[begin..end) of a row list.
+struct HistItem {
+  const uint32_t* rows;  // row list (UNSAMPLED-flagged ids)
+  uint32_t begin, end;
+  uint32_t k;            // class (gradient column)
+  uint32_t root;         // 1: also accumulate the node total
+  void* out;             // HB entries of 16 B (double2 or longlong2)
+  void* total;           // double2* / longlong2* when root
+};
+
+struct HistLaunch {
+  const Ghist* g;
+  const void* gpair;     // FP32: float2 [K][n]; FIXED: uint64 packed [K][n]
+  int fixed;
+  int quant_bits;
+  const HistItem* items; // device
+  const uint64_t* prefix;  // device, exclusive prefix of item lengths, [count+1]
+  const int* count;      // device: number of items
+  int max_items;
+  const FeatureTile* tiles;  // device
+  int ntiles;
+  unsigned long long* rows_done;  // device counter of sampled rows, or null
+};
+
+int hist_prepare(sb_ctx* ctx, Ghist* g);
+int launch_hist(sb_ctx* ctx, const HistLaunch& L);
+int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const int* count,
+                      int max_items);
+int hist_grid(sb_ctx* ctx, const Ghist* g);
+
+// ----------------------------------------------------------------- model
+struct HostTree {
+  std::vector<sb_node> nodes;
+  std::vector<uint32_t> cats;
+};
+
+struct DevEnsemble {
+  DBuf<int4> nodes;          // packed predict nodes
+  DBuf<int> cat_end;         // per node: end of its category list
+  DBuf<int64_t> tree_off;    // node offset per tree
+  DBuf<uint32_t> cats;
+  DBuf<float> weights;
+  DBuf<sb_node> full;        // full nodes (SHAP)
+  DBuf<double> tree_mean;
+  int n_trees = 0;
+  int max_depth = 0;
+};
+
+}  // namespace sb
+
+struct sb_ghist : sb::Ghist {};
+
+struct sb_model {
+  sb_ctx* ctx = nullptr;
+  std::vector<sb::HostTree> trees;
+  std::vector<float> weights;
+  float base_score = 0.0f;
+  int num_class = 0;
+  int n_features = 0;
+  int objective = 0;
+  bool dev_valid = false;
+  sb::DevEnsemble dev;
+};
+
+namespace sb {
+
+int n_outputs(int objective, int num_class);
+int model_upload(sb_model* m);
+
+// ---------------------------------------------------- FP64 split math
+// Written with explicit round-to-nearest intrinsics so that no FMA
+// contraction changes a result bit: the fixed-point path reproduces the CPU
+// oracle's gains exactly. Formulas: tree/gain.rs:78-126 and
+// tree/constraints.rs:70-134.
+struct RegP {
+  double lambda, alpha, mds, mcw;
+};
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ __forceinline__ double threshold_l1(double g, double a) {
+  if (g > a) return dsub(g, a);
+  if (g < -a) return dadd(g, a);
+  return 0.0;
+}
+__device__ __forceinline__ double clampd(double x, double lo, double hi) {
+  if (x < lo) x = lo;
+  if (x > hi) x = hi;
+  return x;
+}
+__device__ __forceinline__ double calc_weight(double g, double h, const RegP& r) {
+  if (h < r.mcw || h <= 0.0) return 0.0;
+  double w = ddiv(-threshold_l1(g, r.alpha), dadd(h, r.lambda));
+  if (r.mds > 0.0) w = clampd(w, -r.mds, r.mds);
+  return w;
+}
+__device__ __forceinline__ double calc_gain(double g, double h, const RegP& r) {
+  if (h < r.mcw || h <= 0.0) return 0.0;
+  double t = threshold_l1(g, r.alpha);
+  if (r.mds == 0.0) return ddiv(dmul(t, t), dadd(h, r.lambda));
+  double w = calc_weight(g, h, r);
+  return -dadd(dmul(dmul(2.0, t), w), dmul(dmul(dadd(h, r.lambda), w), w));
+}
+__device__ __forceinline__ double calc_weight_bounded(double g, double h, const RegP& r, double lo,
+                                                      double hi) {
+  if (h < r.mcw || h <= 0.0) return clampd(0.0, lo, hi);
+  double w = ddiv(-threshold_l1(g, r.alpha), dadd(h, r.lambda));
+  if (r.mds > 0.0) w = clampd(w, -r.mds, r.mds);
+  return clampd(w, lo, hi);
+}
+__device__ __forceinline__ double gain_at_weight(double g, double h, const RegP& r, double w) {
+  if (h < r.mcw || h <= 0.0) return 0.0;
+  double t = threshold_l1(g, r.alpha);
+  return -dadd(dmul(dmul(2.0, t), w), dmul(dmul(dadd(h, r.lambda), w), w));
+}
+__device__ __forceinline__ bool satisfies(int dir, double wl, double wr) {
+  if (dir > 0) return wl <= wr;
+  if (dir < 0) return wl >= wr;
+  return true;
+}
+__device__ __forceinline__ long long total_cmp_key(double x) {
+  long long b = __double_as_longlong(x);
+  b ^= (long long)(((unsigned long long)(b >> 63)) >> 1);
+  return b;
+}
+
+// Rust `f32 as u32`: saturating, NaN -> 0.
+__host__ __device__ __forceinline__ uint32_t f32_as_u32(float v) {
+  if (!(v > 0.0f)) return 0u;
+  if (v >= 4294967296.0f) return 0xFFFFFFFFu;
+  return (uint32_t)v;
+}
+
+// Power-of-two exponent of the fixed-point scale: q = rint(x * 2^s) keeps
+// |q| <= 2^bits for |x| <= m.
+__host__ __device__ __forceinline__ int quant_shift(float m, int bits) {
+  if (!(m > 0.0f) || !(m < INFINITY)) return 0;
+  int e = ilogbf(m);
+  int s = (bits - 1) - e;
+  if (s > 100) s = 100;
+  if (s < -100) s = -100;
+  return s;
+}
+
+// Rows a CTA may fold into its packed 32+32-bit partial before flushing.
+__host__ __device__ __forceinline__ uint32_t fixed_rows_per_flush(int bits) {
+  return (uint32_t)((0x7FFFFFFFull >> bits) - 1ull);
+}
+
+}  // namespace sb

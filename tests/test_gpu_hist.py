@@ -1,0 +1,70 @@
+"""K4/K5 through the HistogramBackend seam (sb_hist_build / sb_hist_subtract)
+against CpuBackend::build of the oracle."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from engines import GpuEngine
+from gpu_helpers import mixed_data, random_gpair
+from kat_checks import check_case
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+CASES = [c for c in json.load(open(os.path.join(HERE, "golden", "reference_kats.json")))["cases"]
+         if c["kind"] in ("hist", "subtract")]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_hist_reference_kats(case, sb, ctx):
+    check_case(case, GpuEngine(sb, ctx), sb.TrainingParams)
+
+
+@pytest.mark.parametrize("n,f,frac", [(2000, 10, 1.0), (60000, 40, 0.7), (200000, 100, 0.5)])
+def test_fp32_within_1e5_of_f64(sb, ctx, orc, n, f, frac):
+    x, _ = mixed_data(n, f, seed=n)
+    g = random_gpair(n, seed=1, logistic=True)
+    rng = np.random.default_rng(2)
+    rows = np.sort(rng.choice(n, int(n * frac), replace=False)).astype(np.uint32)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    got = sb.GpuBackend("fp32", ctx=ctx).build(gh, rows, g)
+    d = orc.data(x)
+    want = d.hist(rows, g, threads=8)
+    mag = d.hist(rows, np.abs(g), threads=8)  # sum of |g| and |h| per bin
+    err = np.abs(got - want)
+    # relative to the bin's absolute mass (1e-5), with an absolute floor for
+    # near-empty bins
+    assert np.all(err <= 1e-5 * mag + 1e-12), float(np.max(err / (mag + 1e-30)))
+
+
+@pytest.mark.parametrize("bits", [12, 16, 20])
+def test_fixed_point_is_exact(sb, ctx, orc, bits):
+    n, f = 100000, 30
+    x, _ = mixed_data(n, f, seed=7, n_cat=2, card=16)
+    ft = np.zeros(f, np.uint8)
+    ft[-2:] = 1
+    g = random_gpair(n, seed=3)
+    rows = np.arange(0, n, 3, dtype=np.uint32)
+    gh = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx)
+    got = sb.GpuBackend("fixed", quantize_bits=bits, ctx=ctx).build(gh, rows, g)
+    gq, _, _ = orc.quantize(g, bits)
+    want = orc.data(x, ft).hist(rows, gq, threads=1)
+    assert np.array_equal(got, want)
+    # and deterministic across calls
+    again = sb.GpuBackend("fixed", quantize_bits=bits, ctx=ctx).build(gh, rows, g)
+    assert np.array_equal(got, again)
+
+
+def test_empty_rows_give_zero_histogram(sb, ctx):
+    x, _ = mixed_data(1000, 5, seed=9)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    out = sb.GpuBackend(ctx=ctx).build(gh, np.zeros(0, np.uint32), random_gpair(1000))
+    assert not out.any()
+
+
+def test_dimension_mismatch_is_reported(sb, ctx):
+    x, _ = mixed_data(100, 5, seed=9)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    with pytest.raises(sb.SbError):
+        sb.GpuBackend(ctx=ctx).build(gh, np.arange(10, dtype=np.uint32), random_gpair(99))

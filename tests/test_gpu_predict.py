@@ -1,0 +1,87 @@
+"""predict_margin / predict / predict_contribs on the GPU against the oracle."""
+import numpy as np
+import pytest
+
+from gpu_helpers import mixed_data
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(orc, x, y, ft=None, **kw):
+    from sequoia_boost_b200 import TrainingParams
+    p = TrainingParams(**kw)
+    r = orc.train(x, y, p, kw.pop("rounds", 20) if "rounds" in kw else 20, ftypes=ft)
+    return p, r["model"].export(), r["model"].base_score
+
+
+@pytest.mark.parametrize("kind", ["regression", "categorical", "multiclass"])
+def test_margins_bit_exact(sb, ctx, orc, kind):
+    ft = None
+    if kind == "categorical":
+        x, ft = mixed_data(8000, 10, seed=3, n_cat=3, card=12)
+    else:
+        x, _ = mixed_data(8000, 10, seed=4)
+    rng = np.random.default_rng(5)
+    if kind == "multiclass":
+        y = rng.integers(0, 4, len(x)).astype(np.float32)
+        kw = dict(objective="multi:softprob", num_class=4, max_depth=4, eta=0.3)
+    else:
+        y = (np.nan_to_num(x[:, 0]) * 2 + rng.standard_normal(len(x))).astype(np.float32)
+        kw = dict(objective="reg:squarederror", max_depth=6, eta=0.2)
+    p, arrays, base = _model(orc, x, y, ft, **kw)
+    k = p.num_class if kind == "multiclass" else 0
+    m = sb.BoostedModel.from_arrays(*arrays[:4], base, k, x.shape[1], objective=p.objective, ctx=ctx)
+    xt, _ = mixed_data(3000, 10, seed=99, n_cat=3 if kind == "categorical" else 0, card=14)
+    got = m.predict_margin(sb.DMatrix(xt))
+    want = orc.predict_margin(arrays, xt, base, k)
+    assert np.array_equal(got, want)
+    for lim in (1, 7):
+        got = m.predict_margin_limited(sb.DMatrix(xt), lim)
+        want = orc.predict_margin(arrays, xt, base, k, ntree_limit=lim)
+        assert np.array_equal(got, want)
+    pr = m.predict(sb.DMatrix(xt))
+    assert np.allclose(pr, orc.transform(p.objective, want, max(k, 0)), rtol=1e-6, atol=1e-7)
+
+
+def test_base_margin_overrides_base_score(sb, ctx, orc):
+    x, _ = mixed_data(2000, 6, seed=6)
+    y = np.random.default_rng(1).standard_normal(2000).astype(np.float32)
+    p, arrays, base = _model(orc, x, y, max_depth=4)
+    m = sb.BoostedModel.from_arrays(*arrays[:4], base, 0, 6, ctx=ctx)
+    bm = np.linspace(-1, 1, 2000).astype(np.float32)
+    got = m.predict_margin(sb.DMatrix(x, base_margin=bm))
+    want = orc.predict_margin(arrays, x, base, 0, base_margin=bm)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("multiclass", [False, True])
+def test_contribs_match_oracle_and_add_up(sb, ctx, orc, multiclass):
+    x, _ = mixed_data(1500, 8, seed=7)
+    rng = np.random.default_rng(2)
+    if multiclass:
+        y = rng.integers(0, 3, len(x)).astype(np.float32)
+        kw = dict(objective="multi:softprob", num_class=3, max_depth=4, eta=0.3)
+        k = 3
+    else:
+        y = (np.nan_to_num(x[:, 1]) - np.nan_to_num(x[:, 2]) + 0.1 * rng.standard_normal(len(x)))
+        y = y.astype(np.float32)
+        kw = dict(objective="reg:squarederror", max_depth=6, eta=0.3)
+        k = 0
+    p, arrays, base = _model(orc, x, y, **kw)
+    m = sb.BoostedModel.from_arrays(*arrays[:4], base, k, 8, objective=p.objective, ctx=ctx)
+    got = m.predict_contribs(sb.DMatrix(x))
+    want = orc.predict_contribs(arrays, x, base, k)
+    assert np.max(np.abs(got - want)) < 1e-4
+    kk = max(k, 1)
+    margin = orc.predict_margin(arrays, x, base, k).reshape(len(x), kk)
+    sums = got.reshape(len(x), kk, 9).astype(np.float64).sum(axis=2)
+    assert np.max(np.abs(sums - margin)) < 1e-4
+
+
+def test_dimension_mismatch(sb, ctx, orc):
+    x, _ = mixed_data(500, 6, seed=6)
+    y = np.zeros(500, np.float32)
+    p, arrays, base = _model(orc, x, y, max_depth=2)
+    m = sb.BoostedModel.from_arrays(*arrays[:4], base, 0, 6, ctx=ctx)
+    with pytest.raises(sb.SbError):
+        m.predict_margin(sb.DMatrix(x[:, :5]))
