@@ -572,7 +572,7 @@ __device__ Chosen scan_feature(const BState& S, const char* H, int k, int f, con
         res.cand = chosen;
       }
     }
-    if (MODE == 0) res.gain = fmax_g;
+    if (MODE == 0) res.gain = warp_max(fmax_g);  // every lane's candidates
     return res;
   }
   // ---- categorical (evaluate_categorical, hist.rs:607-653)
@@ -697,7 +697,7 @@ __device__ Chosen scan_feature(const BState& S, const char* H, int k, int f, con
       }
     }
   }
-  if (MODE == 0) res.gain = fmax_g;
+  if (MODE == 0) res.gain = warp_max(fmax_g);
   return res;
 }
 

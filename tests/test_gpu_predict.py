@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 def _model(orc, x, y, ft=None, **kw):
     from sequoia_boost_b200 import TrainingParams
     p = TrainingParams(**kw)
-    r = orc.train(x, y, p, kw.pop("rounds", 20) if "rounds" in kw else 20, ftypes=ft)
+    r = orc.train(x, y, p, 20, ftypes=ft)
     return p, r["model"].export(), r["model"].base_score
 
 
@@ -33,14 +33,14 @@ def test_margins_bit_exact(sb, ctx, orc, kind):
     m = sb.BoostedModel.from_arrays(*arrays[:4], base, k, x.shape[1], objective=p.objective, ctx=ctx)
     xt, _ = mixed_data(3000, 10, seed=99, n_cat=3 if kind == "categorical" else 0, card=14)
     got = m.predict_margin(sb.DMatrix(xt))
-    want = orc.predict_margin(arrays, xt, base, k)
-    assert np.array_equal(got, want)
+    full = orc.predict_margin(arrays, xt, base, k)
+    assert np.array_equal(got, full)
     for lim in (1, 7):
         got = m.predict_margin_limited(sb.DMatrix(xt), lim)
         want = orc.predict_margin(arrays, xt, base, k, ntree_limit=lim)
         assert np.array_equal(got, want)
     pr = m.predict(sb.DMatrix(xt))
-    assert np.allclose(pr, orc.transform(p.objective, want, max(k, 0)), rtol=1e-6, atol=1e-7)
+    assert np.allclose(pr, orc.transform(p.objective, full, max(k, 0)), rtol=1e-6, atol=1e-7)
 
 
 def test_base_margin_overrides_base_score(sb, ctx, orc):

@@ -33,7 +33,7 @@ VARIANTS = {
     "deep_subset": dict(max_depth=8, lambda_=0.5),
     "colsample": dict(max_depth=6, colsample_bytree=0.8, colsample_bylevel=0.7, colsample_bynode=0.8,
                       seed=11),
-    "regularised": dict(max_depth=5, alpha=0.3, max_delta_step=0.7, gamma=0.05, min_child_weight=3.0),
+    "regularised": dict(max_depth=5, alpha=0.3, max_delta_step=4.0, gamma=0.05, min_child_weight=3.0),
     "monotone": dict(max_depth=6, monotone_constraints=[1, -1, 0, 1]),
     "interaction": dict(max_depth=6, interaction_constraints=[[0, 1, 2], [3, 4], [5, 6, 7, 8]]),
 }
