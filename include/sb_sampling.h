@@ -85,13 +85,12 @@ SB_HD uint64_t sb_splitmix_bounded(sb_splitmix* g, uint64_t n) {
 }
 
 /*
- * subsample(pool, ratio): in place on `idx[0..len)`; returns the new length.
- * Same steps as tree/sampler.rs:60-70 and train.rs:479-489: ratio >= 1 or
- * len <= 1 keeps the pool; otherwise k = clamp(round(ratio*len), 1, len),
- * Fisher-Yates shuffle from the back (as SliceRandom::shuffle), truncate to k,
- * sort ascending.
+ * Fisher-Yates shuffle from the back (as SliceRandom::shuffle) followed by a
+ * truncation to k = clamp(round(ratio*len), 1, len); returns k. The first k
+ * entries are the sample, in shuffled order. ratio >= 1 or len <= 1 keeps
+ * the pool and draws nothing.
  */
-SB_HD int sb_subsample(uint32_t* idx, int len, double ratio, sb_splitmix* g) {
+SB_HD int sb_shuffle_truncate(uint32_t* idx, int len, double ratio, sb_splitmix* g) {
   if (ratio >= 1.0 || len <= 1) return len;
   /* f64::round and C round() both round half away from zero. */
   long long k = (long long)round(ratio * (double)len);
@@ -101,14 +100,24 @@ SB_HD int sb_subsample(uint32_t* idx, int len, double ratio, sb_splitmix* g) {
     int j = (int)sb_splitmix_bounded(g, (uint64_t)(i + 1));
     uint32_t t = idx[i]; idx[i] = idx[j]; idx[j] = t;
   }
-  /* insertion sort of the first k (k <= a few hundred features) */
-  for (int i = 1; i < (int)k; ++i) {
+  return (int)k;
+}
+
+/*
+ * subsample(pool, ratio): in place on `idx[0..len)`; returns the new length.
+ * Same steps as tree/sampler.rs:60-70 and train.rs:479-489: shuffle, truncate,
+ * sort ascending.
+ */
+SB_HD int sb_subsample(uint32_t* idx, int len, double ratio, sb_splitmix* g) {
+  if (ratio >= 1.0 || len <= 1) return len;
+  int k = sb_shuffle_truncate(idx, len, ratio, g);
+  for (int i = 1; i < k; ++i) { /* insertion sort (pools are small) */
     uint32_t v = idx[i];
     int j = i - 1;
     while (j >= 0 && idx[j] > v) { idx[j + 1] = idx[j]; --j; }
     idx[j + 1] = v;
   }
-  return (int)k;
+  return k;
 }
 
 #endif /* SB_SAMPLING_H */

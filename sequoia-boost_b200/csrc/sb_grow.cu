@@ -15,7 +15,7 @@
 // One boosting round is a fixed sequence of kernels whose work sizes live in
 // device memory (no host round trip inside a round):
 //   k_gradient -> k_round_prep -> [k_quantize] -> root histograms ->
-//   per level d: k_eval -> k_assign -> k_partition -> k_plan -> histograms
+//   per level d: k_eval_scan -> k_eval_pick -> k_assign -> k_partition -> k_plan -> histograms
 //   -> k_round_end.
 // All frontier nodes of all K class trees are processed by each launch.
 #include <algorithm>
@@ -27,7 +27,7 @@ namespace sb {
 namespace {
 
 constexpr double K_RT_EPS = 1e-6;  // hist.rs:22
-constexpr int PART_TILE = 2048;    // rows per partition tile
+constexpr int PART_TILE = 4096;    // rows per partition tile
 constexpr int EVAL_THREADS = 256;
 
 struct NodeSplit {
@@ -47,6 +47,8 @@ struct NodeSplit {
 struct Fill {
   unsigned int left, right, lsamp, rsamp;
 };
+
+struct FeatRec;
 
 struct BState {
   // shapes
@@ -121,10 +123,16 @@ struct BState {
   int4* ptiles;
   int* ptile_count;
   int ptile_cap;
+  FeatRec* frec;            // [K][maxw][F] phase-2a summaries
   // sampling
-  uint32_t* pool;           // [K][F]
+  uint32_t* pool;           // [K][F] the tree's colsample_bytree pool, ascending
   int* pool_len;            // [K]
+  uint32_t* upool;          // [K][F] pool features with >= 2 bins, ascending
+  int* upool_len;           // [K]
+  uint32_t* pool_mask;      // [K][FW] bitmask of upool
+  const uint32_t* usable;   // [FW] features with >= 2 bins
   uint32_t* samp_scratch;   // [1024][F] when per-node sampling is on
+  double* mbuf;             // [K][maxw][F] phase-1 best gain per (node, feature)
   // outputs
   sb_node* out_nodes;       // [tree_cap][maxn]
   uint32_t* out_cats;       // [tree_cap][cat_cap]
@@ -265,37 +273,94 @@ __global__ void k_gradient(BState S) {
 }
 
 // Column subset of node `nid` (sampler.rs:52-70 with sb_sampling.h keys),
-// intersected with the node's allowed set, as a bitmask.
+// intersected with the tree's usable pool and the node's allowed set, as a
+// bitmask written word by word.
 __device__ void node_feature_mask(const BState& S, int k, int nid, uint64_t tkey, uint32_t* out,
                                   const uint32_t* allowed, bool allowed_all, uint32_t* scratch) {
-  for (int w = 0; w < S.FW; ++w) out[w] = 0u;
-  const uint32_t* pool = S.pool + (size_t)k * S.F;
-  int len = S.pool_len[k];
+  const uint32_t* pm = S.pool_mask + (size_t)k * S.FW;
   if (S.bylevel >= 1.0 && S.bynode >= 1.0) {
-    for (int i = 0; i < len; ++i) out[pool[i] >> 5] |= 1u << (pool[i] & 31);
-  } else {
-    for (int i = 0; i < len; ++i) scratch[i] = pool[i];
-    sb_splitmix gen{sb_node_key(tkey, (uint64_t)nid)};
-    int l1 = sb_subsample(scratch, len, S.bylevel, &gen);
-    int l2 = sb_subsample(scratch, l1, S.bynode, &gen);
-    for (int i = 0; i < l2; ++i) out[scratch[i] >> 5] |= 1u << (scratch[i] & 31);
+    for (int w = 0; w < S.FW; ++w) out[w] = pm[w] & (allowed_all ? 0xFFFFFFFFu : allowed[w]);
+    return;
   }
-  if (!allowed_all)
-    for (int w = 0; w < S.FW; ++w) out[w] &= allowed[w];
+  const uint32_t* pool = S.pool + (size_t)k * S.F;
+  const int len = S.pool_len[k];
+  for (int i = 0; i < len; ++i) scratch[i] = pool[i];
+  sb_splitmix gen{sb_node_key(tkey, (uint64_t)nid)};
+  int l1 = sb_subsample(scratch, len, S.bylevel, &gen);
+  int l2 = sb_subsample(scratch, l1, S.bynode, &gen);
+  int p = 0;
+  for (int w = 0; w < S.FW; ++w) {
+    uint32_t word = 0u;
+    while (p < l2 && (int)(scratch[p] >> 5) == w) {
+      word |= 1u << (scratch[p] & 31);
+      ++p;
+    }
+    out[w] = word & pm[w] & (allowed_all ? 0xFFFFFFFFu : allowed[w]);
+  }
 }
 
-// Per round: quantisation scales, the sampled-row fallback, the per-tree
-// column pools and the root of every class tree.
-__global__ void k_round_prep(BState S) {
+// Per round, one CTA per class tree: quantisation scales, the sampled-row
+// fallback, the tree's colsample_bytree pool (train.rs:479-489) and its root.
+constexpr int PREP_THREADS = 128;
+__global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
+  __shared__ uint32_t s_a[4096];
+  __shared__ uint32_t s_b[4096];
+  __shared__ uint32_t s_mask[128];
+  __shared__ int s_len;
   const unsigned long long round = *S.round + S.round_base;
-  const int tid = threadIdx.x;
-  if (tid == 0) *S.qerr = 0ull;
-  if (tid == 0 && *S.kept == 0 && !S.ext_gpair) {  // train.rs:472-474
-    uint64_t rk = sb_round_key(S.seed, round);
-    S.rows0[sb_row_fallback(rk, S.n)] &= ~UNSAMPLED;
-    *S.kept = 1;
+  const int k = blockIdx.x, tid = threadIdx.x;
+  const int F = S.F;
+  const uint64_t tkey = sb_tree_key(S.seed, round, (uint64_t)(k + S.k_base));
+  if (k == 0 && tid == 0) {
+    *S.qerr = 0ull;
+    if (*S.kept == 0 && !S.ext_gpair) {  // train.rs:472-474
+      uint64_t rk = sb_round_key(S.seed, round);
+      S.rows0[sb_row_fallback(rk, S.n)] &= ~UNSAMPLED;
+      *S.kept = 1;
+    }
   }
-  for (int k = tid; k < S.K; k += blockDim.x) {
+  for (int f = tid; f < F; f += blockDim.x) s_a[f] = (uint32_t)f;
+  for (int w = tid; w < S.FW; w += blockDim.x) s_mask[w] = 0u;
+  __syncthreads();
+  if (tid == 0) {
+    int len = F;
+    if (S.bytree < 1.0) {
+      sb_splitmix gen{tkey};
+      len = sb_shuffle_truncate(s_a, F, S.bytree, &gen);
+    }
+    s_len = len;
+  }
+  __syncthreads();
+  const int len = s_len;
+  // sort the sample ascending: rank of each (distinct) feature id
+  for (int i = tid; i < len; i += blockDim.x) {
+    uint32_t v = s_a[i];
+    int r = 0;
+    for (int j = 0; j < len; ++j) r += s_a[j] < v ? 1 : 0;
+    s_b[r] = v;
+  }
+  __syncthreads();
+  uint32_t* pool = S.pool + (size_t)k * F;
+  for (int i = tid; i < len; i += blockDim.x) {
+    uint32_t f = s_b[i];
+    pool[i] = f;
+    if ((S.usable[f >> 5] >> (f & 31)) & 1u) atomicOr(&s_mask[f >> 5], 1u << (f & 31));
+  }
+  __syncthreads();
+  for (int w = tid; w < S.FW; w += blockDim.x) S.pool_mask[(size_t)k * S.FW + w] = s_mask[w];
+  if (tid == 0) {  // usable pool list, ascending
+    int u = 0;
+    uint32_t* up = S.upool + (size_t)k * F;
+    for (int w = 0; w < S.FW; ++w) {
+      uint32_t word = s_mask[w];
+      while (word) {
+        int b = __ffs(word) - 1;
+        word &= word - 1;
+        up[u++] = (uint32_t)(w * 32 + b);
+      }
+    }
+    S.upool_len[k] = u;
+    S.pool_len[k] = len;
     if (S.fixed) {
       int sg = quant_shift(__uint_as_float(S.maxabs[2 * k]), S.bits);
       int sh = quant_shift(__uint_as_float(S.maxabs[2 * k + 1]), S.bits);
@@ -304,22 +369,12 @@ __global__ void k_round_prep(BState S) {
       S.inv_scale[2 * k] = ldexp(1.0, -sg);
       S.inv_scale[2 * k + 1] = ldexp(1.0, -sh);
     }
-    // colsample_bytree pool (train.rs:479-489)
-    uint64_t tkey = sb_tree_key(S.seed, round, (uint64_t)(k + S.k_base));
-    uint32_t* pool = S.pool + (size_t)k * S.F;
-    for (int f = 0; f < S.F; ++f) pool[f] = (uint32_t)f;
-    int len = S.F;
-    if (S.bytree < 1.0) {
-      sb_splitmix gen{tkey};
-      len = sb_subsample(pool, S.F, S.bytree, &gen);
-    }
-    S.pool_len[k] = len;
     S.num_nodes[k] = 1;
     S.lvl_begin[k] = 0;
     S.lvl_count[k] = 1;
     S.prev_begin[k] = 0;
     S.cat_count[k] = 0;
-    size_t r0 = NI(S, k, 0);
+    const size_t r0 = NI(S, k, 0);
     S.seg[r0] = make_uint2(0u, (unsigned)S.n);
     S.nsamp[r0] = *S.kept;
     S.bounds[r0] = make_double2(-INFINITY, INFINITY);
@@ -327,8 +382,6 @@ __global__ void k_round_prep(BState S) {
     S.built[r0] = 1;
     S.parent[r0] = -1;
     S.root_total[k] = make_longlong2(0, 0);
-    node_feature_mask(S, k, 0, tkey, S.fmask + r0 * S.FW, nullptr, true,
-                      S.samp_scratch ? S.samp_scratch + (size_t)tid * S.F : nullptr);
     HistItem it;
     it.rows = S.rows0;  // level 0 shares the root list of class 0
     it.begin = 0;
@@ -339,11 +392,15 @@ __global__ void k_round_prep(BState S) {
     it.total = &S.root_total[k];
     S.items[k] = it;
     S.prefix[k] = (uint64_t)k * S.n;
+    if (k == 0) {
+      S.prefix[S.K] = (uint64_t)S.K * S.n;
+      *S.item_count = S.K;
+    }
   }
-  if (tid == 0) {
-    S.prefix[S.K] = (uint64_t)S.K * S.n;
-    *S.item_count = S.K;
-  }
+  __syncthreads();
+  if (tid == 0)  // after the pool mask is published
+    node_feature_mask(S, k, 0, tkey, S.fmask + NI(S, k, 0) * S.FW, nullptr, true,
+                      S.samp_scratch ? S.samp_scratch + (size_t)k * S.F : nullptr);
 }
 
 // FIXED: q = rint(x * 2^s), packed (q_g << 32) + q_h.
@@ -437,419 +494,434 @@ struct CatScratch {
   double h[MAX_CAT_BINS];
   long long key[MAX_CAT_BINS];
   uint16_t ne[MAX_CAT_BINS];      // non-empty bins, ascending
-  uint16_t order[MAX_CAT_BINS];   // sorted by ratio (stable)
+  uint16_t order[MAX_CAT_BINS];   // positions into ne/g/h, sorted by ratio (stable)
 };
 
-// The result of a sequential replay of one feature.
+constexpr int AMB_MAX = 6;  // ambiguous records kept per (node, feature)
+
+// Phase-2 summary of one feature of one node (see k_eval_records).
+struct FeatRec {
+  double def_gain;          // gain of the last certain record
+  int def_idx;              // its candidate index, -1 none
+  int namb;                 // ambiguous records after it (AMB_MAX + 1 = overflow)
+  double amb_gain[AMB_MAX];
+  int amb_idx[AMB_MAX];
+};
+
 struct Chosen {
   double gain;
   int cand;    // candidate index within the feature, -1 none
 };
 
-// Warp-parallel scan of one feature's candidates in the reference's order:
-//   numeric  : bins ascending, direction A (missing right) before B
-//   category : prefixes of the ratio-sorted non-empty bins
-// MODE 0 returns the feature's max candidate gain (phase 1).
-// MODE 1 replays `consider`'s rule `g > best + 1e-6` exactly from state
-// b_in: a taken candidate must be a strict new prefix maximum P; any
-// candidate with g > P + eps is certainly taken; so the outcome is the last
-// certain record k*, followed by a short sequential resolution of the
-// remaining (ambiguous) records after k*.
+enum { SCAN_MAX = 0, SCAN_REPLAY = 1, SCAN_RECORDS = 2, SCAN_EXTRACT = 3 };
+
+// Warp-parallel walk over one feature's candidates in the reference's order:
+//   numeric  : bins ascending, direction A (missing right) before direction B
+//              (missing left, only when the node has missing values);
+//              candidate index 2*i + dir
+//   category : prefixes of the non-empty bins sorted by G/(H+lambda)
+//              (evaluate_categorical, hist.rs:607-653); candidate index = prefix
+// Modes:
+//   SCAN_MAX     the feature's best candidate gain
+//   SCAN_RECORDS with the prefix maximum P started at `b_in` (the best gain of
+//                earlier features, or 0): the last candidate with g > P + eps
+//                (certainly taken by consider's rule g > best + 1e-6) and the
+//                ambiguous records after it (P < g <= P + eps)
+//   SCAN_REPLAY  consider's sequential rule from state b_in (exact fallback)
+//   SCAN_EXTRACT statistics of candidate `want` into *out
 template <int MODE>
 __device__ Chosen scan_feature(const BState& S, const char* H, int k, int f, const EvalNode& E,
-                               double b_in, CatScratch* cs, double* s_gains, NodeSplit* out) {
+                               double b_in, CatScratch* cs, double* s_gains, NodeSplit* out,
+                               FeatRec* rec = nullptr, int want = -1) {
   const int lane = threadIdx.x & 31;
   const int fs = (int)S.foff[f], nb = (int)S.foff[f + 1] - fs;
   const int dir = S.mono ? S.mono[f] : 0;
-  Chosen res{b_in, -1};
-  double fmax_g = -INFINITY;
-  if (!S.is_cat[f]) {
-    // missing statistics come from the feature's missing bin; present = sum
-    double2 miss = hist_entry(S, H, S.total_bins + f, k);
-    double pg = 0.0, ph = 0.0;
+  const bool cat = S.is_cat[f] != 0;
+  double2 miss = make_double2(0.0, 0.0);
+  double pg = 0.0, ph = 0.0;
+  int ncand;   // candidate positions (bins or prefixes)
+  bool has_missing = false;
+  if (!cat) {
+    miss = hist_entry(S, H, S.total_bins + f, k);  // missing statistics: the missing bin
     for (int c0 = 0; c0 < nb; c0 += 32) {
-      int i = c0 + lane;
-      double2 v = i < nb ? hist_entry(S, H, fs + i, k) : make_double2(0.0, 0.0);
+      const int i = c0 + lane;
+      const double2 v = i < nb ? hist_entry(S, H, fs + i, k) : make_double2(0.0, 0.0);
       pg += v.x;
       ph += v.y;
     }
     pg = warp_sum(pg);
     ph = warp_sum(ph);
-    const bool has_missing = miss.y > 1e-6;
-    for (int pass = 0; pass < (MODE == 0 ? 1 : 2); ++pass) {
-      double cg = 0.0, ch = 0.0, P = b_in;
-      // pass 0 (MODE 1): last certain record; pass 1: resolution
-      __shared__ int s_kstar[EVAL_THREADS / 32];
-      __shared__ double s_gstar[EVAL_THREADS / 32];
-      const int w = threadIdx.x >> 5;
-      if (pass == 0 && lane == 0) {
-        s_kstar[w] = -1;
-        s_gstar[w] = b_in;
+    has_missing = miss.y > 1e-6;
+    ncand = nb - 1;
+  } else {
+    const double lam = S.reg.lambda;
+    int nne = 0;
+    for (int c0 = 0; c0 < nb; c0 += 32) {
+      const int i = c0 + lane;
+      const double2 v = i < nb ? hist_entry(S, H, fs + i, k) : make_double2(0.0, -1.0);
+      const bool ne = i < nb && v.y > 0.0;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, ne);
+      if (ne) {
+        const int pos = nne + __popc(m & ((1u << lane) - 1u));
+        cs->ne[pos] = (uint16_t)i;
+        cs->g[pos] = v.x;
+        cs->h[pos] = v.y;
+        cs->key[pos] = total_cmp_key(ddiv(v.x, dadd(v.y, lam)));
       }
-      __syncwarp();
-      int kstar = pass == 1 ? s_kstar[w] : -1;
-      double bstate = pass == 1 ? s_gstar[w] : b_in;
-      int chosen = kstar;
-      for (int c0 = 0; c0 < nb - 1; c0 += 32) {
-        const int i = c0 + lane;
-        double2 v = i < nb ? hist_entry(S, H, fs + i, k) : make_double2(0.0, 0.0);
-        double sg = warp_incl_sum(v.x), shh = warp_incl_sum(v.y);
-        double ag = cg + sg, ah = ch + shh;
-        double tg = __shfl_sync(0xFFFFFFFFu, sg, 31), th = __shfl_sync(0xFFFFFFFFu, shh, 31);
-        double gA = -INFINITY, gB = -INFINITY, wlA = 0, wrA = 0, wlB = 0, wrB = 0;
-        if (i < nb - 1) {
-          gA = cand_gain(S, E, dir, ag, ah, dsub(E.tg, ag), dsub(E.th, ah), &wlA, &wrA);
-          if (has_missing)
-            gB = cand_gain(S, E, dir, dadd(ag, miss.x), dadd(ah, miss.y), dsub(pg, ag), dsub(ph, ah),
-                           &wlB, &wrB);
-        }
-        if (MODE == 0) {
-          fmax_g = fmax(fmax_g, fmax(gA, gB));
-        } else {
-          double lm = fmax(gA, gB);
-          double PA = warp_excl_max(lm, P);
-          double PB = fmax(PA, gA);
-          if (pass == 0) {
-            int ci = -1;
-            double cgain = 0;
-            if (gB > PB + K_RT_EPS) { ci = 2 * i + 1; cgain = gB; }
-            else if (gA > PA + K_RT_EPS) { ci = 2 * i; cgain = gA; }
-            // the highest candidate index wins
-            int best_ci = ci;
-            for (int o = 16; o > 0; o >>= 1) best_ci = max(best_ci, __shfl_xor_sync(0xFFFFFFFFu, best_ci, o));
-            if (best_ci >= 0 && ci == best_ci) {
-              s_kstar[w] = ci;
-              s_gstar[w] = cgain;
-            }
-            __syncwarp();
-          } else {
-            // records after k* in candidate order, resolved sequentially
-            bool recA = (2 * i > kstar) && gA > PA;
-            bool recB = (2 * i + 1 > kstar) && gB > PB;
-            unsigned ma = __ballot_sync(0xFFFFFFFFu, recA), mb = __ballot_sync(0xFFFFFFFFu, recB);
-            s_gains[lane] = gA;
-            s_gains[32 + lane] = gB;
-            __syncwarp();
-            if (lane == 0 && (ma | mb)) {
-              for (int L = 0; L < 32; ++L) {
-                if ((ma >> L) & 1u) {
-                  double gv = s_gains[L];
-                  if (gv > bstate + K_RT_EPS) { bstate = gv; chosen = 2 * (c0 + L); }
-                }
-                if ((mb >> L) & 1u) {
-                  double gv = s_gains[32 + L];
-                  if (gv > bstate + K_RT_EPS) { bstate = gv; chosen = 2 * (c0 + L) + 1; }
-                }
-              }
-            }
-            bstate = __shfl_sync(0xFFFFFFFFu, bstate, 0);
-            chosen = __shfl_sync(0xFFFFFFFFu, chosen, 0);
-            __syncwarp();
-            // the owner of the chosen candidate records its statistics
-            if (out && chosen >= 0 && (chosen >> 1) == i) {
-              const bool isB = chosen & 1;
-              out->feature = f;
-              out->bin = i;
-              out->default_left = isB ? 1 : 0;
-              out->is_cat = 0;
-              out->ncat = 0;
-              out->lg = isB ? dadd(ag, miss.x) : ag;
-              out->lh = isB ? dadd(ah, miss.y) : ah;
-              out->rg = isB ? dsub(pg, ag) : dsub(E.tg, ag);
-              out->rh = isB ? dsub(ph, ah) : dsub(E.th, ah);
-              out->wl = isB ? wlB : wlA;
-              out->wr = isB ? wrB : wrA;
-            }
-            __syncwarp();
-          }
-          P = fmax(P, warp_max(lm));
-        }
-        cg += tg;
-        ch += th;
-      }
-      if (MODE == 1 && pass == 1) {
-        res.gain = bstate;
-        res.cand = chosen;
-      }
-    }
-    if (MODE == 0) res.gain = warp_max(fmax_g);  // every lane's candidates
-    return res;
-  }
-  // ---- categorical (evaluate_categorical, hist.rs:607-653)
-  const double lam = S.reg.lambda;
-  int nne = 0;
-  for (int c0 = 0; c0 < nb; c0 += 32) {
-    int i = c0 + lane;
-    double2 v = i < nb ? hist_entry(S, H, fs + i, k) : make_double2(0.0, -1.0);
-    bool ne = i < nb && v.y > 0.0;
-    unsigned m = __ballot_sync(0xFFFFFFFFu, ne);
-    if (ne) {
-      int pos = nne + __popc(m & ((1u << lane) - 1u));
-      cs->ne[pos] = (uint16_t)i;
-      cs->g[pos] = v.x;
-      cs->h[pos] = v.y;
-      cs->key[pos] = total_cmp_key(ddiv(v.x, dadd(v.y, lam)));
-    }
-    nne += __popc(m);
-  }
-  __syncwarp();
-  if (nne < 2) {
-    res.gain = MODE == 0 ? -INFINITY : b_in;
-    return res;
-  }
-  for (int i = lane; i < nne; i += 32) {  // stable rank by key
-    long long ki = cs->key[i];
-    int r = 0;
-    for (int j = 0; j < nne; ++j) {
-      long long kj = cs->key[j];
-      r += (kj < ki || (kj == ki && j < i)) ? 1 : 0;
-    }
-    cs->order[r] = (uint16_t)i;  // index into ne/g/h
-  }
-  __syncwarp();
-  const int ncand = nne - 1;
-  __shared__ int s_kstar_c[EVAL_THREADS / 32];
-  __shared__ double s_gstar_c[EVAL_THREADS / 32];
-  const int w = threadIdx.x >> 5;
-  for (int pass = 0; pass < (MODE == 0 ? 1 : 2); ++pass) {
-    double cg = 0.0, ch = 0.0, P = b_in;
-    if (pass == 0 && lane == 0) {
-      s_kstar_c[w] = -1;
-      s_gstar_c[w] = b_in;
+      nne += __popc(m);
     }
     __syncwarp();
-    int kstar = pass == 1 ? s_kstar_c[w] : -1;
-    double bstate = pass == 1 ? s_gstar_c[w] : b_in;
-    int chosen = kstar;
-    for (int c0 = 0; c0 < ncand; c0 += 32) {
-      const int pidx = c0 + lane;
-      double vg = 0.0, vh = 0.0;
-      if (pidx < nne) {
-        int o = cs->order[pidx];
-        vg = cs->g[o];
-        vh = cs->h[o];
+    for (int i = lane; i < nne; i += 32) {  // stable rank by key
+      const long long ki = cs->key[i];
+      int r = 0;
+      for (int j = 0; j < nne; ++j) {
+        const long long kj = cs->key[j];
+        r += (kj < ki || (kj == ki && j < i)) ? 1 : 0;
       }
-      double lg = cg + warp_incl_sum(vg), lh = ch + warp_incl_sum(vh);
-      double tg = __shfl_sync(0xFFFFFFFFu, lg - cg, 31), th = __shfl_sync(0xFFFFFFFFu, lh - ch, 31);
-      double gv = -INFINITY, wl = 0, wr = 0;
-      if (pidx < ncand) gv = cand_gain(S, E, dir, lg, lh, dsub(E.tg, lg), dsub(E.th, lh), &wl, &wr);
-      if (MODE == 0) {
-        fmax_g = fmax(fmax_g, gv);
-      } else {
-        double Pc = warp_excl_max(gv, P);
-        if (pass == 0) {
-          int ci = gv > Pc + K_RT_EPS ? pidx : -1;
-          int best_ci = ci;
-          for (int o = 16; o > 0; o >>= 1) best_ci = max(best_ci, __shfl_xor_sync(0xFFFFFFFFu, best_ci, o));
-          if (best_ci >= 0 && ci == best_ci) {
-            s_kstar_c[w] = ci;
-            s_gstar_c[w] = gv;
+      cs->order[r] = (uint16_t)i;
+    }
+    __syncwarp();
+    ncand = nne - 1;  // prefixes leaving at least one category right
+  }
+  Chosen res{MODE == SCAN_MAX ? -INFINITY : b_in, -1};
+  if (ncand <= 0) {
+    if (MODE == SCAN_RECORDS && lane == 0) {
+      rec->def_idx = -1;
+      rec->namb = 0;
+    }
+    return res;
+  }
+
+  double run_max = -INFINITY;  // SCAN_MAX
+  double P = b_in;             // prefix maximum (RECORDS / REPLAY)
+  int def_idx = -1;            // RECORDS: last certain record
+  double def_gain = 0.0;
+  int namb = 0;                // RECORDS: ambiguous records after def_idx (lane 0's copy)
+  double bstate = b_in;        // REPLAY
+  int chosen = -1;
+  double cg = 0.0, ch = 0.0;   // running prefix of the bins walked so far
+  for (int c0 = 0; c0 < ncand; c0 += 32) {
+    const int i = c0 + lane;   // candidate position
+    double vg = 0.0, vh = 0.0;
+    if (!cat) {
+      if (i < nb) {
+        const double2 v = hist_entry(S, H, fs + i, k);
+        vg = v.x;
+        vh = v.y;
+      }
+    } else if (i <= ncand) {
+      const int o = cs->order[i];
+      vg = cs->g[o];
+      vh = cs->h[o];
+    }
+    const double ag = cg + warp_incl_sum(vg), ah = ch + warp_incl_sum(vh);
+    const double tg = __shfl_sync(0xFFFFFFFFu, ag - cg, 31), th = __shfl_sync(0xFFFFFFFFu, ah - ch, 31);
+    double gA = -INFINITY, gB = -INFINITY, wlA = 0, wrA = 0, wlB = 0, wrB = 0;
+    if (i < ncand) {
+      gA = cand_gain(S, E, dir, ag, ah, dsub(E.tg, ag), dsub(E.th, ah), &wlA, &wrA);
+      if (!cat && has_missing)
+        gB = cand_gain(S, E, dir, dadd(ag, miss.x), dadd(ah, miss.y), dsub(pg, ag), dsub(ph, ah), &wlB, &wrB);
+    }
+    const double lm = fmax(gA, gB);
+    if (MODE == SCAN_MAX) {
+      run_max = fmax(run_max, lm);
+    } else if (MODE == SCAN_EXTRACT) {
+      if (out && (want >> (cat ? 0 : 1)) == i) {
+        const bool isB = !cat && (want & 1);
+        out->feature = f;
+        out->bin = cat ? 0 : i;
+        out->default_left = isB ? 1 : 0;
+        out->is_cat = cat ? 1 : 0;
+        out->ncat = cat ? i + 1 : 0;
+        out->lg = isB ? dadd(ag, miss.x) : ag;
+        out->lh = isB ? dadd(ah, miss.y) : ah;
+        out->rg = isB ? dsub(pg, ag) : dsub(E.tg, ag);
+        out->rh = isB ? dsub(ph, ah) : dsub(E.th, ah);
+        out->wl = isB ? wlB : wlA;
+        out->wr = isB ? wrB : wrA;
+      }
+      if ((want >> (cat ? 0 : 1)) < c0 + 32) break;
+    } else {
+      const double PA = warp_excl_max(lm, P);  // prefix max before candidate 2i (or i)
+      const double PB = fmax(PA, gA);          // before candidate 2i+1
+      const int step = cat ? 1 : 2;
+      if (MODE == SCAN_RECORDS) {
+        int ci = -1;
+        double cgain = 0.0;
+        if (!cat && gB > PB + K_RT_EPS) { ci = 2 * i + 1; cgain = gB; }
+        else if (gA > PA + K_RT_EPS) { ci = step * i; cgain = gA; }
+        int best_ci = ci;
+        for (int o = 16; o > 0; o >>= 1) best_ci = max(best_ci, __shfl_xor_sync(0xFFFFFFFFu, best_ci, o));
+        if (best_ci >= 0) {
+          const int owner = cat ? best_ci - c0 : (best_ci >> 1) - c0;
+          def_gain = __shfl_sync(0xFFFFFFFFu, cgain, owner);
+          def_idx = best_ci;
+          namb = 0;  // earlier ambiguous records are no longer after the last certain one
+        }
+        const bool ambA = step * i > def_idx && gA > PA && !(gA > PA + K_RT_EPS);
+        const bool ambB = !cat && 2 * i + 1 > def_idx && gB > PB && !(gB > PB + K_RT_EPS);
+        const unsigned ma = __ballot_sync(0xFFFFFFFFu, ambA), mb = __ballot_sync(0xFFFFFFFFu, ambB);
+        if (ma | mb) {
+          s_gains[lane] = gA;
+          s_gains[32 + lane] = gB;
+          __syncwarp();
+          if (lane == 0) {
+            for (int L = 0; L < 32; ++L) {
+              for (int d2 = 0; d2 < 2; ++d2) {
+                if (!(((d2 ? mb : ma) >> L) & 1u)) continue;
+                if (namb < AMB_MAX) {
+                  rec->amb_gain[namb] = s_gains[d2 * 32 + L];
+                  rec->amb_idx[namb] = cat ? c0 + L : 2 * (c0 + L) + d2;
+                }
+                namb++;
+              }
+            }
           }
           __syncwarp();
-        } else {
-          bool rec = pidx > kstar && gv > Pc;
-          unsigned m = __ballot_sync(0xFFFFFFFFu, rec);
-          s_gains[lane] = gv;
+        }
+      } else {  // SCAN_REPLAY: consider's rule, candidates in order, from bstate
+        const bool rA = gA > PA, rB = !cat && gB > PB;  // only records can be taken
+        const unsigned ma = __ballot_sync(0xFFFFFFFFu, rA), mb = __ballot_sync(0xFFFFFFFFu, rB);
+        if (ma | mb) {
+          s_gains[lane] = gA;
+          s_gains[32 + lane] = gB;
           __syncwarp();
-          if (lane == 0 && m) {
+          if (lane == 0) {
             for (int L = 0; L < 32; ++L)
-              if ((m >> L) & 1u) {
-                double x = s_gains[L];
-                if (x > bstate + K_RT_EPS) { bstate = x; chosen = c0 + L; }
+              for (int d2 = 0; d2 < 2; ++d2) {
+                if (!(((d2 ? mb : ma) >> L) & 1u)) continue;
+                const double gv = s_gains[d2 * 32 + L];
+                if (gv > bstate + K_RT_EPS) {
+                  bstate = gv;
+                  chosen = cat ? c0 + L : 2 * (c0 + L) + d2;
+                }
               }
           }
           bstate = __shfl_sync(0xFFFFFFFFu, bstate, 0);
           chosen = __shfl_sync(0xFFFFFFFFu, chosen, 0);
           __syncwarp();
-          if (out && chosen == pidx) {
-            out->feature = f;
-            out->bin = 0;
-            out->default_left = 0;
-            out->is_cat = 1;
-            out->ncat = pidx + 1;
-            out->lg = lg;
-            out->lh = lh;
-            out->rg = dsub(E.tg, lg);
-            out->rh = dsub(E.th, lh);
-            out->wl = wl;
-            out->wr = wr;
-          }
-          __syncwarp();
         }
-        P = fmax(P, warp_max(gv));
       }
-      cg += tg;
-      ch += th;
+      P = fmax(P, warp_max(lm));
     }
-    if (MODE == 1 && pass == 1) {
-      res.gain = bstate;
-      res.cand = chosen;
-      if (out && chosen >= 0 && chosen == res.cand) {
-        // categories routed left, in sweep order (cats_left, hist.rs:630-636)
-        for (int i = lane; i < MAX_CAT_BINS / 32; i += 32) out->cat_mask[i] = 0u;
-        __syncwarp();
-        for (int p = lane; p <= chosen; p += 32) {
-          int b = cs->ne[cs->order[p]];
-          out->cat_order[p] = (uint8_t)b;
-          atomicOr(&out->cat_mask[b >> 5], 1u << (b & 31));
-        }
-        __syncwarp();
-      }
-    }
+    cg += tg;
+    ch += th;
   }
-  if (MODE == 0) res.gain = warp_max(fmax_g);
+  if (MODE == SCAN_MAX) res.gain = warp_max(run_max);
+  if (MODE == SCAN_RECORDS && lane == 0) {
+    rec->def_idx = def_idx;
+    rec->def_gain = def_gain;
+    rec->namb = namb > AMB_MAX ? AMB_MAX + 1 : namb;
+  }
+  if (MODE == SCAN_REPLAY) {
+    res.gain = bstate;
+    res.cand = chosen;
+  }
+  if (MODE == SCAN_EXTRACT && cat && out) {
+    // categories routed left, in sweep order (cats_left, hist.rs:630-636)
+    for (int i = lane; i < MAX_CAT_BINS / 32; i += 32) out->cat_mask[i] = 0u;
+    __syncwarp();
+    for (int p = lane; p <= want; p += 32) {
+      const int b = cs->ne[cs->order[p]];
+      out->cat_order[p] = (uint8_t)b;
+      atomicOr(&out->cat_mask[b >> 5], 1u << (b & 31));
+    }
+    __syncwarp();
+  }
   return res;
 }
 
-// One CTA per frontier node: materialise a subtracted histogram if the node
-// was not built, then find its best split with the reference's tie rule.
-__global__ void __launch_bounds__(EVAL_THREADS) k_eval(BState S, int d) {
+// Evaluation context of a frontier node: its total, monotone bounds and the
+// parent gain of evaluate() (hist.rs:445-457).
+__device__ EvalNode eval_node(const BState& S, int k, size_t ni, int d) {
+  double2 st;
+  if (d == 0) {  // root statistics, summed by the root histogram launch
+    if (S.fixed) {
+      longlong2 q = S.root_total[k];
+      st = make_double2(dmul((double)q.x, S.inv_scale[2 * k]), dmul((double)q.y, S.inv_scale[2 * k + 1]));
+    } else {
+      st = reinterpret_cast<const double2*>(S.root_total)[k];
+    }
+  } else {
+    st = S.stats[ni];
+  }
+  const double2 bd = S.bounds[ni];
+  EvalNode E;
+  E.tg = st.x;
+  E.th = st.y;
+  E.lo = bd.x;
+  E.hi = bd.y;
+  E.parent_gain = S.constrained
+      ? gain_at_weight(st.x, st.y, S.reg, calc_weight_bounded(st.x, st.y, S.reg, bd.x, bd.y))
+      : calc_gain(st.x, st.y, S.reg);
+  return E;
+}
+
+constexpr int SCAN_WARPS = EVAL_THREADS / 32;
+
+__device__ __forceinline__ bool in_mask(const uint32_t* m, int f) { return (m[f >> 5] >> (f & 31)) & 1u; }
+
+// Phase 1, one warp per (frontier node, usable pool feature): materialise the
+// feature's bins of a node whose histogram is the parent's minus the built
+// sibling's (the subtraction trick, K5), then record the feature's best
+// candidate gain (-inf when the node may not use the feature).
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) {
   extern __shared__ double ev_sm[];
-  const int k = blockIdx.y, slot = blockIdx.x;
+  const int slot = blockIdx.x, k = blockIdx.z;
   if (slot >= S.lvl_count[k]) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pi = blockIdx.y * SCAN_WARPS + warp;
+  if (pi >= S.upool_len[k]) return;
+  const int f = (int)S.upool[(size_t)k * S.F + pi];
   const int nid = S.lvl_begin[k] + slot;
   const size_t ni = NI(S, k, nid);
   char* H = level_hist(S, d, k, slot);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-  double* s_M = ev_sm;                                    // [F]
-  int* s_flist = reinterpret_cast<int*>(s_M + S.F);       // [F]
-  double* s_gains = reinterpret_cast<double*>(s_flist + S.F + (S.F & 1));  // [64]
-  CatScratch* s_cat = reinterpret_cast<CatScratch*>(s_gains + 64);        // [nwarps] if categorical
-  __shared__ int s_nf;
-  __shared__ EvalNode s_E;
-  __shared__ NodeSplit s_best;
-
-  if (d > 0 && !S.built[ni]) {  // sibling = parent - built child (K5)
+  if (d > 0 && !S.built[ni]) {
     const int pslot = S.parent[ni] - S.prev_begin[k];
     const char* P = level_hist(S, d - 1, k, pslot);
     const char* B = level_hist(S, d, k, slot ^ 1);
-    if (S.fixed) {
-      const longlong2* p = reinterpret_cast<const longlong2*>(P);
-      const longlong2* b = reinterpret_cast<const longlong2*>(B);
-      longlong2* o = reinterpret_cast<longlong2*>(H);
-      for (int i = tid; i < S.HB; i += blockDim.x) {
-        longlong2 x = p[i], y = b[i];
-        o[i] = make_longlong2(x.x - y.x, x.y - y.y);
-      }
-    } else {
-      const double2* p = reinterpret_cast<const double2*>(P);
-      const double2* b = reinterpret_cast<const double2*>(B);
-      double2* o = reinterpret_cast<double2*>(H);
-      for (int i = tid; i < S.HB; i += blockDim.x) {
-        double2 x = p[i], y = b[i];
-        o[i] = make_double2(dsub(x.x, y.x), dsub(x.y, y.y));
-      }
-    }
-    __syncthreads();
-  }
-  if (tid == 0) {
-    if (d == 0) {  // root statistics, summed by the root histogram launch
-      double2 t;
+    const int fs = (int)S.foff[f], nb = (int)S.foff[f + 1] - fs;
+    for (int i = lane; i <= nb; i += 32) {
+      const int e = i < nb ? fs + i : S.total_bins + f;  // bins, then the missing bin
       if (S.fixed) {
-        longlong2 q = S.root_total[k];
-        t = make_double2(dmul((double)q.x, S.inv_scale[2 * k]), dmul((double)q.y, S.inv_scale[2 * k + 1]));
+        longlong2 x = reinterpret_cast<const longlong2*>(P)[e], y = reinterpret_cast<const longlong2*>(B)[e];
+        reinterpret_cast<longlong2*>(H)[e] = make_longlong2(x.x - y.x, x.y - y.y);
       } else {
-        t = reinterpret_cast<const double2*>(S.root_total)[k];
+        double2 x = reinterpret_cast<const double2*>(P)[e], y = reinterpret_cast<const double2*>(B)[e];
+        reinterpret_cast<double2*>(H)[e] = make_double2(dsub(x.x, y.x), dsub(x.y, y.y));
       }
-      S.stats[ni] = t;
     }
-    double2 st = S.stats[ni];
-    double2 bd = S.bounds[ni];
-    EvalNode E;
-    E.tg = st.x;
-    E.th = st.y;
-    E.lo = bd.x;
-    E.hi = bd.y;
-    E.parent_gain = S.constrained
-        ? gain_at_weight(st.x, st.y, S.reg, calc_weight_bounded(st.x, st.y, S.reg, bd.x, bd.y))
-        : calc_gain(st.x, st.y, S.reg);
-    s_E = E;
-    s_best.loss_chg = 0.0;
-    s_best.feature = -1;
-    s_best.valid = 0;
-    s_best.ncat = 0;
-    s_best.is_cat = 0;
-    s_best.default_left = 1;
-    s_best.wl = s_best.wr = 0.0;
-    s_best.lg = s_best.lh = s_best.rg = s_best.rh = 0.0;
-    s_best.bin = 0;
+    __syncwarp();
   }
-  // candidate features: sampled & allowed, with >= 2 bins, ascending
-  if (warp == 0) {
-    const uint32_t* fm = S.fmask + ni * S.FW;
-    int cnt = 0;
-    for (int w0 = 0; w0 < S.FW; w0 += 32) {
-      int wi = w0 + lane;
-      uint32_t word = wi < S.FW ? fm[wi] : 0u;
-      // keep features with >= 2 bins
-      for (int b = 0; b < 32 && word; ++b) {
-        if ((word >> b) & 1u) {
-          int f = wi * 32 + b;
-          if (f >= S.F || S.foff[f + 1] - S.foff[f] < 2) word &= ~(1u << b);
-        }
-      }
-      int pc = __popc(word);
-      int incl = pc;
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      int pos = cnt + incl - pc;
-      while (word) {
-        int b = __ffs(word) - 1;
-        word &= word - 1;
-        s_flist[pos++] = wi * 32 + b;
-      }
-      cnt += __shfl_sync(0xFFFFFFFFu, incl, 31);
+  double m = -INFINITY;
+  if (in_mask(S.fmask + ni * S.FW, f)) {
+    const EvalNode E = eval_node(S, k, ni, d);
+    CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+    m = scan_feature<SCAN_MAX>(S, H, k, f, E, 0.0, cs, nullptr, nullptr).gain;
+  }
+  if (lane == 0) S.mbuf[((size_t)k * S.maxw + slot) * S.F + f] = m;
+}
+
+// Phase 2a, one warp per (frontier node, usable pool feature): with Q = the
+// best gain of the node's earlier features (or 0), find this feature's last
+// certain record and its ambiguous records (FeatRec).
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) {
+  extern __shared__ double ev_sm[];
+  __shared__ double s_gains[SCAN_WARPS][64];
+  const int slot = blockIdx.x, k = blockIdx.z;
+  if (slot >= S.lvl_count[k]) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pi = blockIdx.y * SCAN_WARPS + warp;
+  if (pi >= S.upool_len[k]) return;
+  const int f = (int)S.upool[(size_t)k * S.F + pi];
+  const int nid = S.lvl_begin[k] + slot;
+  const size_t ni = NI(S, k, nid);
+  const size_t ri = ((size_t)k * S.maxw + slot) * S.F + f;
+  FeatRec* rec = S.frec + ri;
+  const double* M = S.mbuf + ((size_t)k * S.maxw + slot) * S.F;
+  if (!(M[f] > K_RT_EPS)) {  // no candidate can be taken from any state >= 0
+    if (lane == 0) {
+      rec->def_idx = -1;
+      rec->namb = 0;
     }
-    if (lane == 0) s_nf = cnt;
+    return;
   }
-  __syncthreads();
-  const EvalNode E = s_E;
-  const int nf = s_nf;
-  CatScratch* my_cs = S.cat_cap > 0 ? s_cat + warp : nullptr;
-  // phase 1: every feature's max candidate gain
-  for (int i = warp; i < nf; i += nwarps) {
-    Chosen c = scan_feature<0>(S, H, k, s_flist[i], E, 0.0, my_cs, nullptr, nullptr);
-    if (lane == 0) s_M[i] = c.gain;
+  const uint32_t* fm = S.fmask + ni * S.FW;
+  double q = 0.0;  // max over the node's earlier features (only masked slots are current)
+  for (int j = lane; j < f; j += 32)
+    if (in_mask(fm, j)) q = fmax(q, M[j]);
+  q = warp_max(q);
+  const EvalNode E = eval_node(S, k, ni, d);
+  CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+  scan_feature<SCAN_RECORDS>(S, level_hist(S, d, k, slot), k, f, E, q, cs, s_gains[warp], nullptr, rec);
+}
+
+// Phase 2b, one warp per frontier node: the winner of consider's sequential
+// rule is the last certain record over all features, followed by a short
+// sequential resolution over the ambiguous records after it.
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
+  extern __shared__ double ev_sm[];
+  __shared__ NodeSplit s_best[SCAN_WARPS];
+  __shared__ double s_gains[SCAN_WARPS][64];
+  const int k = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = blockIdx.x * SCAN_WARPS + warp;
+  if (slot >= S.lvl_count[k]) return;
+  const int nid = S.lvl_begin[k] + slot;
+  const size_t ni = NI(S, k, nid);
+  const char* H = level_hist(S, d, k, slot);
+  const EvalNode E = eval_node(S, k, ni, d);
+  NodeSplit* best = &s_best[warp];
+  const double* M = S.mbuf + ((size_t)k * S.maxw + slot) * S.F;
+  const FeatRec* R = S.frec + ((size_t)k * S.maxw + slot) * S.F;
+  const uint32_t* fm = S.fmask + ni * S.FW;
+  CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+  // last feature holding a certain record
+  int fstar = -1;
+  for (int j = lane; j < S.F; j += 32)
+    if (in_mask(fm, j) && M[j] > K_RT_EPS && R[j].def_idx >= 0) fstar = j;
+  for (int o = 16; o > 0; o >>= 1) fstar = max(fstar, __shfl_xor_sync(0xFFFFFFFFu, fstar, o));
+  double b = 0.0;
+  int cf = -1, cidx = -1;
+  if (fstar >= 0) {
+    b = R[fstar].def_gain;
+    cf = fstar;
+    cidx = R[fstar].def_idx;
   }
-  __syncthreads();
-  // phase 2: exact sequential replay over the features that can still win
-  if (warp == 0) {
-    double b = 0.0;
-    for (int i = 0; i < nf; ++i) {
-      if (!(s_M[i] > b + K_RT_EPS)) continue;
-      Chosen c = scan_feature<1>(S, H, k, s_flist[i], E, b, my_cs, s_gains, &s_best);
+  // ambiguous records after the winner, in candidate order (lane-uniform walk)
+  for (int f = fstar < 0 ? 0 : fstar; f < S.F; ++f) {
+    if (!in_mask(fm, f) || !(M[f] > K_RT_EPS)) continue;
+    const FeatRec& r = R[f];
+    if (r.namb == 0) continue;
+    if (r.namb > AMB_MAX) {  // overflow: exact replay of this feature from b
+      Chosen c = scan_feature<SCAN_REPLAY>(S, H, k, f, E, b, cs, s_gains[warp], nullptr);
       if (c.cand >= 0) {
         b = c.gain;
-        if (lane == 0) s_best.loss_chg = b;
+        cf = f;
+        cidx = c.cand;
       }
-      __syncwarp();
+      continue;
     }
+    for (int a = 0; a < r.namb; ++a)
+      if (r.amb_gain[a] > b + K_RT_EPS) {
+        b = r.amb_gain[a];
+        cf = f;
+        cidx = r.amb_idx[a];
+      }
   }
-  __syncthreads();
-  if (tid == 0) {
-    NodeSplit& o = S.split[ni];
-    bool found = s_best.feature >= 0 && s_best.loss_chg > K_RT_EPS;
-    bool valid = found && s_best.loss_chg > S.gamma && s_best.lh >= S.reg.mcw && s_best.rh >= S.reg.mcw;
-    o.loss_chg = s_best.loss_chg;
-    o.lg = s_best.lg;
-    o.lh = s_best.lh;
-    o.rg = s_best.rg;
-    o.rh = s_best.rh;
-    o.wl = s_best.wl;
-    o.wr = s_best.wr;
-    o.feature = s_best.feature;
-    o.bin = s_best.bin;
-    o.default_left = s_best.default_left;
-    o.is_cat = s_best.is_cat;
-    o.ncat = s_best.is_cat ? s_best.ncat : 0;
+  if (lane == 0) {
+    best->feature = -1;
+    best->is_cat = 0;
+    best->ncat = 0;
+    best->default_left = 1;
+    best->bin = 0;
+    best->lg = best->lh = best->rg = best->rh = 0.0;
+    best->wl = best->wr = 0.0;
+    if (d == 0) S.stats[ni] = make_double2(E.tg, E.th);
+  }
+  __syncwarp();
+  if (cf >= 0) scan_feature<SCAN_EXTRACT>(S, H, k, cf, E, 0.0, cs, nullptr, best, nullptr, cidx);
+  __syncwarp();
+  NodeSplit& o = S.split[ni];
+  if (lane == 0) {
+    const bool found = cf >= 0 && b > K_RT_EPS;
+    const bool valid = found && b > S.gamma && best->lh >= S.reg.mcw && best->rh >= S.reg.mcw;
+    o.loss_chg = found ? b : 0.0;
+    o.lg = best->lg;
+    o.lh = best->lh;
+    o.rg = best->rg;
+    o.rh = best->rh;
+    o.wl = best->wl;
+    o.wr = best->wr;
+    o.feature = best->feature;
+    o.bin = best->bin;
+    o.default_left = best->default_left;
+    o.is_cat = best->is_cat;
+    o.ncat = best->is_cat ? best->ncat : 0;
     o.valid = valid ? 1 : 0;
   }
-  if (s_best.is_cat && s_best.feature >= 0) {
-    NodeSplit& o = S.split[ni];
-    for (int i = tid; i < MAX_CAT_BINS / 32; i += blockDim.x) o.cat_mask[i] = s_best.cat_mask[i];
-    for (int i = tid; i < s_best.ncat; i += blockDim.x) o.cat_order[i] = s_best.cat_order[i];
+  if (cf >= 0 && best->is_cat) {
+    for (int i = lane; i < MAX_CAT_BINS / 32; i += 32) o.cat_mask[i] = best->cat_mask[i];
+    for (int i = lane; i < best->ncat; i += 32) o.cat_order[i] = best->cat_order[i];
   }
 }
 
@@ -1007,76 +1079,85 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
   if (tid == 0) *S.ptile_count = min(s_tile_carry, S.ptile_cap);
 }
 
-// K7 + K8: stable-count partition of every split node's rows into its two
-// children (left rows fill from the segment start, right rows from its end),
-// and the margin update (train.rs:326-328) for rows whose node is final.
-__global__ void __launch_bounds__(256) k_partition(BState S, int d) {
+// K7 + K8: partition every split node's rows into its two children (left rows
+// fill the segment from its start, right rows from its end; order is kept
+// within a tile), and the margin update (train.rs:326-328) for rows whose node
+// is final. Each thread owns 16 consecutive positions of a 4096-row tile, so
+// 16 independent bin loads are in flight per thread; one packed block scan
+// gives every thread its left / right offsets.
+constexpr int PART_THREADS = 256;
+constexpr int PART_PER = PART_TILE / PART_THREADS;
+__global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
   __shared__ unsigned int sm_u[33];
   __shared__ unsigned int s_base[2];
   const bool last = (d + 1 == S.max_depth);
   const int ntiles = *S.ptile_count;
   const uint32_t* rows_cur_all = (d & 1) ? S.rows1 : S.rows0;
   uint32_t* rows_nxt_all = (d & 1) ? S.rows0 : S.rows1;
+  const int K = S.K;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tile = S.ptiles[t];
     const int k = tile.x, nid = tile.y;
     const size_t ni = NI(S, k, nid);
     const uint32_t* rows_cur = rows_cur_all + (d == 0 ? 0 : (size_t)k * S.n);
     uint32_t* rows_nxt = rows_nxt_all + (size_t)k * S.n;
-    const NodeSplit& sp = S.split[ni];
-    const int K = S.K;
-    if (!sp.valid) {
+    const int valid = S.split[ni].valid;
+    const int p0 = tile.z + threadIdx.x * PART_PER;
+    const int pe = min(tile.w, p0 + PART_PER);
+    if (!valid) {  // a final leaf: its rows take the leaf value
       const float lv = S.leafval[ni];
-      for (int p = tile.z + threadIdx.x; p < tile.w; p += blockDim.x) {
-        uint32_t rv = rows_cur[p];
-        uint32_t id = rv & ~UNSAMPLED;
+      for (int p = p0; p < pe; ++p) {
+        const uint32_t rv = rows_cur[p];
+        const uint32_t id = rv & ~UNSAMPLED;
         if (S.update_margin) S.margin[(size_t)id * K + k] += lv;
         if (S.row_leaf) S.row_leaf[id] = (rv & UNSAMPLED) ? -1 : nid;
       }
       continue;
     }
+    const NodeSplit& sp = S.split[ni];
     const int f = sp.feature, sbin = sp.bin, dl = sp.default_left, isc = sp.is_cat;
     const int left_id = S.out_nodes[((size_t)(*S.round) * K + k) * S.maxn + nid].left;
-    constexpr int PER = PART_TILE / 256;
-    uint32_t rv[PER];
-    bool gl[PER];
+    uint32_t rv[PART_PER];
+    uint16_t bv[PART_PER];
+#pragma unroll
+    for (int q = 0; q < PART_PER; ++q) rv[q] = (p0 + q < pe) ? rows_cur[p0 + q] : UNSAMPLED;
+#pragma unroll
+    for (int q = 0; q < PART_PER; ++q)
+      bv[q] = (p0 + q < pe) ? S.bins[(size_t)(rv[q] & ~UNSAMPLED) * S.Fp + f] : (uint16_t)0;
+    unsigned goleft = 0u;  // bit q: position p0+q goes left
     unsigned nl = 0, nls = 0, nrs = 0;
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      int p = tile.z + q * 256 + threadIdx.x;
-      rv[q] = UNSAMPLED;
-      gl[q] = false;
-      if (p < tile.w) {
-        rv[q] = rows_cur[p];
-        uint32_t id = rv[q] & ~UNSAMPLED;
-        uint16_t b = S.bins[(size_t)id * S.Fp + f];
-        bool go;
-        if (b == MISSING_BIN) go = dl != 0;
-        else if (isc) go = (sp.cat_mask[b >> 5] >> (b & 31)) & 1u;
-        else go = (int)b <= sbin;
-        gl[q] = go;
-        if (last) {
-          int child = go ? left_id : left_id + 1;
-          size_t ci = NI(S, k, child);
-          if (S.update_margin) S.margin[(size_t)id * K + k] += S.leafval[ci];
-          if (S.row_leaf) S.row_leaf[id] = (rv[q] & UNSAMPLED) ? -1 : child;
-        } else {
-          nl += go ? 1u : 0u;
-          bool smp = !(rv[q] & UNSAMPLED);
-          nls += (go && smp) ? 1u : 0u;
-          nrs += (!go && smp) ? 1u : 0u;
-        }
-      }
+    for (int q = 0; q < PART_PER; ++q) {
+      if (p0 + q >= pe) continue;
+      const uint16_t b = bv[q];
+      bool go;
+      if (b == MISSING_BIN) go = dl != 0;
+      else if (isc) go = (sp.cat_mask[b >> 5] >> (b & 31)) & 1u;
+      else go = (int)b <= sbin;
+      const bool smp = !(rv[q] & UNSAMPLED);
+      goleft |= (go ? 1u : 0u) << q;
+      nl += go ? 1u : 0u;
+      nls += (go && smp) ? 1u : 0u;
+      nrs += (!go && smp) ? 1u : 0u;
     }
-    if (last) continue;
-    const int nvalid = min(PART_TILE, tile.w - tile.z);
-    unsigned totl;
-    const unsigned loff = block_scan_excl<unsigned>(nl, &totl, sm_u);
-    unsigned cnt_here = 0;
-#pragma unroll
-    for (int q = 0; q < PER; ++q) cnt_here += (tile.z + q * 256 + (int)threadIdx.x < tile.w) ? 1u : 0u;
-    unsigned totall;
-    const unsigned aoff = block_scan_excl<unsigned>(cnt_here, &totall, sm_u);
+    if (last) {  // children are final leaves: margins only
+      const size_t li = NI(S, k, left_id), ri = li + 1;
+      const float lv = S.leafval[li], rvv = S.leafval[ri];
+      for (int q = 0; q < PART_PER; ++q) {
+        if (p0 + q >= pe) continue;
+        const uint32_t id = rv[q] & ~UNSAMPLED;
+        const bool go = (goleft >> q) & 1u;
+        if (S.update_margin) S.margin[(size_t)id * K + k] += go ? lv : rvv;
+        if (S.row_leaf) S.row_leaf[id] = (rv[q] & UNSAMPLED) ? -1 : (go ? left_id : left_id + 1);
+      }
+      continue;
+    }
+    const unsigned nhere = (unsigned)max(0, pe - p0);
+    // one scan over (positions, left) packed as 16 + 16 bits (tile <= 4096)
+    unsigned tot;
+    const unsigned pre = block_scan_excl<unsigned>((nhere << 16) | nl, &tot, sm_u);
+    const unsigned loff = pre & 0xFFFFu, aoff = pre >> 16;
+    const unsigned totl = tot & 0xFFFFu, totall = tot >> 16;
     unsigned ls = nls, rs = nrs;
     for (int o = 16; o > 0; o >>= 1) {
       ls += __shfl_xor_sync(0xFFFFFFFFu, ls, o);
@@ -1087,23 +1168,20 @@ __global__ void __launch_bounds__(256) k_partition(BState S, int d) {
       if (ls) atomicAdd(&fl->lsamp, ls);
       if (rs) atomicAdd(&fl->rsamp, rs);
     }
-    const unsigned totr = (unsigned)nvalid - totl;
+    const unsigned totr = totall - totl;
     if (threadIdx.x == 0) {
       s_base[0] = atomicAdd(&fl->left, totl);
       s_base[1] = atomicAdd(&fl->right, totr);
     }
     __syncthreads();
     const uint2 sg = S.seg[ni];
-    unsigned li = loff, ri = aoff - loff;  // right rows before mine = all before - left before
-    const unsigned lbase = sg.x + s_base[0];
-    const unsigned rbase = sg.y - s_base[1] - totr;
+    unsigned li = sg.x + s_base[0] + loff;
+    unsigned ri = sg.y - s_base[1] - totr + (aoff - loff);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      int p = tile.z + q * 256 + threadIdx.x;
-      if (p < tile.w) {
-        if (gl[q]) rows_nxt[lbase + li++] = rv[q];
-        else rows_nxt[rbase + ri++] = rv[q];
-      }
+    for (int q = 0; q < PART_PER; ++q) {
+      if (p0 + q >= pe) continue;
+      if ((goleft >> q) & 1u) rows_nxt[li++] = rv[q];
+      else rows_nxt[ri++] = rv[q];
     }
     __syncthreads();
   }
@@ -1261,8 +1339,10 @@ struct sb_booster {
   sb::DBuf<int> d_item_count;
   sb::DBuf<int4> d_ptiles;
   sb::DBuf<int> d_ptile_count;
-  sb::DBuf<uint32_t> d_pool;
-  sb::DBuf<int> d_pool_len;
+  sb::DBuf<uint32_t> d_pool, d_upool, d_pool_mask, d_usable;
+  sb::DBuf<int> d_pool_len, d_upool_len;
+  sb::DBuf<double> d_mbuf;
+  sb::DBuf<sb::FeatRec> d_frec;
   sb::DBuf<uint32_t> d_samp;
   sb::DBuf<sb_node> d_out_nodes;
   sb::DBuf<uint32_t> d_out_cats;
@@ -1457,6 +1537,18 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   SB_TRY(b->d_ptile_count.alloc(ctx, 1));
   SB_TRY(b->d_pool.alloc(ctx, (size_t)K * F));
   SB_TRY(b->d_pool_len.alloc(ctx, K));
+  SB_TRY(b->d_upool.alloc(ctx, (size_t)K * F));
+  SB_TRY(b->d_upool_len.alloc(ctx, K));
+  SB_TRY(b->d_pool_mask.alloc(ctx, (size_t)K * FW));
+  SB_TRY(b->d_mbuf.alloc(ctx, (size_t)K * b->maxw * F));
+  SB_TRY(b->d_frec.alloc(ctx, (size_t)K * b->maxw * F));
+  {
+    std::vector<uint32_t> usable(FW, 0u);
+    for (int f = 0; f < F; ++f)
+      if (g->h_foff[f + 1] - g->h_foff[f] >= 2) usable[f >> 5] |= 1u << (f & 31);
+    SB_TRY(b->d_usable.alloc(ctx, FW));
+    SB_CUDA(cudaMemcpyAsync(b->d_usable.p, usable.data(), FW * 4, cudaMemcpyHostToDevice, st));
+  }
   if (p->colsample_bylevel < 1.0 || p->colsample_bynode < 1.0) SB_TRY(b->d_samp.alloc(ctx, (size_t)1024 * F));
   SB_TRY(b->d_tiles.alloc(ctx, g->tiles.size()));
   SB_CUDA(cudaMemcpyAsync(b->d_tiles.p, g->tiles.data(), g->tiles.size() * sizeof(FeatureTile),
@@ -1541,6 +1633,12 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.ptile_cap = ptile_cap;
   S.pool = b->d_pool.p;
   S.pool_len = b->d_pool_len.p;
+  S.upool = b->d_upool.p;
+  S.upool_len = b->d_upool_len.p;
+  S.pool_mask = b->d_pool_mask.p;
+  S.usable = b->d_usable.p;
+  S.mbuf = b->d_mbuf.p;
+  S.frec = b->d_frec.p;
   S.samp_scratch = b->d_samp.p;
   S.row_leaf = nullptr;
   SB_TRY(booster_alloc_trees(b, K * 16));
@@ -1548,9 +1646,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
 }
 
 size_t eval_smem(const sb_booster* b) {
-  size_t s = (size_t)b->S.F * 8 + (size_t)(b->S.F + 2) * 4 + 64 * 8 + 16;
-  if (b->S.cat_cap) s += (EVAL_THREADS / 32) * sizeof(CatScratch);
-  return s;
+  return b->S.cat_cap ? (EVAL_THREADS / 32) * sizeof(CatScratch) : 0;
 }
 
 int booster_round(sb_booster* b) {
@@ -1568,7 +1664,7 @@ int booster_round(sb_booster* b) {
   }
   const unsigned gblocks = (unsigned)std::min<size_t>((b->n + 255) / 256, (size_t)ctx->num_sms * 16);
   SB_LAUNCH(ctx, k_gradient, gblocks, 256, 0, S);
-  SB_LAUNCH(ctx, k_round_prep, 1, 32, 0, S);
+  SB_LAUNCH(ctx, k_round_prep, (unsigned)b->K, PREP_THREADS, 0, S);
   if (S.fixed) SB_LAUNCH(ctx, k_quantize, gblocks, 256, 0, S);
   HistLaunch L;
   L.g = b->g;
@@ -1581,6 +1677,7 @@ int booster_round(sb_booster* b) {
   L.tiles = b->d_tiles.p;
   L.ntiles = (int)b->g->tiles.size();
   L.rows_done = b->timing ? b->d_hist_rows.p : nullptr;
+  L.pool_mask = S.pool_mask;
   const size_t esm = eval_smem(b);
   auto hist = [&](int max_items) -> int {
     L.max_items = max_items;
@@ -1602,11 +1699,15 @@ int booster_round(sb_booster* b) {
   };
   SB_TRY(hist(b->K));
   for (int d = 0; d < b->D; ++d) {
-    dim3 eg((unsigned)std::min(1 << d, b->maxw), (unsigned)b->K);
-    SB_LAUNCH(ctx, k_eval, eg, EVAL_THREADS, esm, S, d);
+    const unsigned width = (unsigned)std::min(1 << d, b->maxw);
+    dim3 sg(width, (unsigned)((b->g->F + SCAN_WARPS - 1) / SCAN_WARPS), (unsigned)b->K);
+    SB_LAUNCH(ctx, k_eval_scan, sg, EVAL_THREADS, esm, S, d);
+    SB_LAUNCH(ctx, k_eval_records, sg, EVAL_THREADS, esm, S, d);
+    dim3 pg((width + SCAN_WARPS - 1) / SCAN_WARPS, (unsigned)b->K);
+    SB_LAUNCH(ctx, k_eval_pick, pg, EVAL_THREADS, esm, S, d);
     SB_LAUNCH(ctx, k_assign, 1, 1024, 0, S, d, 1);
     unsigned pblocks = (unsigned)ctx->num_sms * 8;
-    SB_LAUNCH(ctx, k_partition, pblocks, 256, 0, S, d);
+    SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
     if (d + 1 < b->D) {
       SB_LAUNCH(ctx, k_plan, 1, 1024, 0, S, d);
       SB_TRY(hist(b->K * (1 << d)));
@@ -1651,8 +1752,10 @@ int booster_collect_timing(sb_booster* b) {
 }  // namespace
 
 int booster_set_eval_smem(sb_booster* b) {
-  size_t esm = eval_smem(b);
-  SB_CUDA(cudaFuncSetAttribute(k_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm));
+  int esm = (int)eval_smem(b);
+  SB_CUDA(cudaFuncSetAttribute(k_eval_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
+  SB_CUDA(cudaFuncSetAttribute(k_eval_pick, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
+  SB_CUDA(cudaFuncSetAttribute(k_eval_records, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
   return SB_OK;
 }
 

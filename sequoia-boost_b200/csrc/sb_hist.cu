@@ -25,9 +25,9 @@
 namespace sb {
 namespace {
 
-constexpr int HIST_THREADS = 1024;
+constexpr int HIST_THREADS = 768;
 constexpr int MAX_TILE_FEATURES = 128;  // 4 features per lane
-constexpr int ROWS_PER_WARP = 4;        // rows in flight per warp
+constexpr int ROWS_PER_WARP = 8;        // rows in flight per warp
 
 struct HistDev {
   const uint16_t* bins;
@@ -43,6 +43,8 @@ struct HistDev {
   int ntiles;
   uint32_t flush_rows;   // FIXED: max rows per shared partial
   unsigned long long* rows_done;  // sampled rows accumulated (or null)
+  const uint32_t* pool_mask;      // [K][FW] features to accumulate (or null: all)
+  int FW;
 };
 
 __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
@@ -54,12 +56,15 @@ __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint
   return lo;
 }
 
+// The shared partial is two planes of nent 32-bit words, g then h (FIXED:
+// int32 / uint32 integers; FP32: floats), so a warp's atomics spread over all
+// 32 banks. Every entry costs one add into each plane.
 template <bool FIXED>
 __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
   extern __shared__ unsigned long long sh_u64[];
-  float* sh_f = reinterpret_cast<float*>(sh_u64);
+  unsigned* sh_g = reinterpret_cast<unsigned*>(sh_u64);
   __shared__ double s_tot_d[2];
-  __shared__ unsigned long long s_tot_u;
+  __shared__ unsigned long long s_tot_u[2];
 
   const int count = *a.count;
   if (count <= 0) return;
@@ -85,83 +90,99 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     const FeatureTile tile = a.tiles[t];
     const int nf = tile.f1 - tile.f0;
     const int nent = tile.nbins + nf;
+    unsigned* sh_h = sh_g + nent;
     const bool want_total = item.root && t == 0;
 
-    // per-lane features of this tile
-    int lbase[4], lmiss[4], lf[4];
+    // lane `lane` owns the 4 consecutive features f0 + 4*lane .. +3 of the tile
+    // (only those of the tree's column pool); one 8-byte load per row fetches
+    // their 4 bins. Tiles start at multiples of 4 and rows are padded to a
+    // multiple of 8 bins, so the load is aligned and stays inside the row.
+    const int fl0 = 4 * lane;
+    const bool lane_on = fl0 < nf;
+    int lbase[4];
+    bool fon[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      int fl = lane + 32 * j;
-      lf[j] = fl < nf ? tile.f0 + fl : -1;
-      lbase[j] = lf[j] >= 0 ? (int)a.foff[lf[j]] - tile.bin0 : 0;
-      lmiss[j] = tile.nbins + fl;
+      const int fl = fl0 + j;
+      const int f = tile.f0 + fl;
+      bool on = fl < nf;
+      if (on && a.pool_mask && !((a.pool_mask[(size_t)item.k * a.FW + (f >> 5)] >> (f & 31)) & 1u)) on = false;
+      fon[j] = on;
+      lbase[j] = on ? (int)a.foff[f] - tile.bin0 : 0;
     }
-    for (int i = threadIdx.x; i < nent; i += blockDim.x) sh_u64[i] = 0ull;
-    if (threadIdx.x == 0) {
-      s_tot_d[0] = 0.0;
-      s_tot_d[1] = 0.0;
-      s_tot_u = 0ull;
+    for (int i = threadIdx.x; i < 2 * nent; i += blockDim.x) sh_g[i] = 0u;
+    if (threadIdx.x < 2) {
+      s_tot_d[threadIdx.x] = 0.0;
+      s_tot_u[threadIdx.x] = 0ull;
     }
     __syncthreads();
 
     double tg = 0.0, th = 0.0;
-    unsigned long long tq = 0ull;
+    long long tqg = 0;
+    unsigned long long tqh = 0;
     unsigned int nsampled = 0;
     const size_t gcol = (size_t)item.k * a.n;
+    const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
     for (uint32_t p = pbeg + warp * ROWS_PER_WARP; p < pend; p += nwarps * ROWS_PER_WARP) {
       uint32_t rid[ROWS_PER_WARP];
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        uint32_t pp = p + q;
+        const uint32_t pp = p + q;
         rid[q] = pp < pend ? item.rows[pp] : UNSAMPLED;
       }
-      float gg[ROWS_PER_WARP], hh[ROWS_PER_WARP];
-      unsigned long long pk[ROWS_PER_WARP];
-      uint16_t bv[ROWS_PER_WARP][4];
+      uint32_t vg[ROWS_PER_WARP], vh[ROWS_PER_WARP];  // FIXED ints or FP32 float bits
+      uint2 bv[ROWS_PER_WARP];
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
         const bool use = !(rid[q] & UNSAMPLED);
         const size_t id = rid[q] & ~UNSAMPLED;
         if (FIXED) {
-          pk[q] = use ? reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + id] : 0ull;
+          const unsigned long long pk = use ? reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + id] : 0ull;
+          vg[q] = (uint32_t)(pk >> 32);
+          vh[q] = (uint32_t)(pk & 0xFFFFFFFFull);
         } else {
-          float2 v = use ? reinterpret_cast<const float2*>(a.gpair)[gcol + id] : make_float2(0.f, 0.f);
-          gg[q] = v.x;
-          hh[q] = v.y;
+          const float2 v = use ? reinterpret_cast<const float2*>(a.gpair)[gcol + id] : make_float2(0.f, 0.f);
+          vg[q] = __float_as_uint(v.x);
+          vh[q] = __float_as_uint(v.y);
         }
-        const uint16_t* brow = a.bins + id * a.Fp;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) bv[q][j] = (use && lf[j] >= 0) ? __ldg(brow + lf[j]) : (uint16_t)0xFFFEu;
+        bv[q] = (use && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
+                                 : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
       }
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
         if (rid[q] & UNSAMPLED) continue;
         nsampled++;
         if (want_total && lane == 0) {
-          if (FIXED) tq += pk[q];
-          else {
-            tg += (double)gg[q];
-            th += (double)hh[q];
+          if (FIXED) {
+            tqg += (int)vg[q];
+            tqh += vh[q];
+          } else {
+            tg += (double)__uint_as_float(vg[q]);
+            th += (double)__uint_as_float(vh[q]);
           }
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const uint16_t b = bv[q][j];
-          if (b == 0xFFFEu) continue;
-          const int idx = (b == MISSING_BIN) ? lmiss[j] : lbase[j] + b;
+          if (!fon[j]) continue;
+          const uint32_t w = j < 2 ? bv[q].x : bv[q].y;
+          const uint32_t b = (j & 1) ? (w >> 16) : (w & 0xFFFFu);
+          const int idx = (b == MISSING_BIN) ? tile.nbins + fl0 + j : lbase[j] + (int)b;
           if (FIXED) {
-            atomicAdd(&sh_u64[idx], pk[q]);
+            atomicAdd(reinterpret_cast<int*>(sh_g) + idx, (int)vg[q]);
+            atomicAdd(sh_h + idx, vh[q]);
           } else {
-            atomicAdd(&sh_f[2 * idx], gg[q]);
-            atomicAdd(&sh_f[2 * idx + 1], hh[q]);
+            atomicAdd(reinterpret_cast<float*>(sh_g) + idx, __uint_as_float(vg[q]));
+            atomicAdd(reinterpret_cast<float*>(sh_h) + idx, __uint_as_float(vh[q]));
           }
         }
       }
     }
     if (a.rows_done && lane == 0 && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
     if (want_total && lane == 0) {
-      if (FIXED) atomicAdd(&s_tot_u, tq);
-      else {
+      if (FIXED) {
+        atomicAdd(&s_tot_u[0], (unsigned long long)tqg);
+        atomicAdd(&s_tot_u[1], tqh);
+      } else {
         atomicAdd(&s_tot_d[0], tg);
         atomicAdd(&s_tot_d[1], th);
       }
@@ -171,16 +192,13 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     for (int i = threadIdx.x; i < nent; i += blockDim.x) {
       const int gi = i < tile.nbins ? tile.bin0 + i : a.total_bins + tile.f0 + (i - tile.nbins);
       if (FIXED) {
-        unsigned long long v = sh_u64[i];
-        if (v) {
-          unsigned long long hq = v & 0xFFFFFFFFull;
-          long long gq = ((long long)(v - hq)) >> 32;
-          unsigned long long* o = reinterpret_cast<unsigned long long*>(item.out) + 2 * (size_t)gi;
-          if (gq) atomicAdd(o, (unsigned long long)gq);
-          if (hq) atomicAdd(o + 1, hq);
-        }
+        const long long gq = (long long)(int)sh_g[i];
+        const unsigned long long hq = sh_h[i];
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(item.out) + 2 * (size_t)gi;
+        if (gq) atomicAdd(o, (unsigned long long)gq);
+        if (hq) atomicAdd(o + 1, hq);
       } else {
-        float g = sh_f[2 * i], h = sh_f[2 * i + 1];
+        const float g = __uint_as_float(sh_g[i]), h = __uint_as_float(sh_h[i]);
         double* o = reinterpret_cast<double*>(item.out) + 2 * (size_t)gi;
         if (g != 0.0f) atomicAdd(o, (double)g);
         if (h != 0.0f) atomicAdd(o + 1, (double)h);
@@ -188,12 +206,9 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     }
     if (want_total && threadIdx.x == 0) {
       if (FIXED) {
-        unsigned long long v = s_tot_u;
-        unsigned long long hq = v & 0xFFFFFFFFull;
-        long long gq = ((long long)(v - hq)) >> 32;
         unsigned long long* o = reinterpret_cast<unsigned long long*>(item.total);
-        atomicAdd(o, (unsigned long long)gq);
-        atomicAdd(o + 1, hq);
+        atomicAdd(o, s_tot_u[0]);
+        atomicAdd(o + 1, s_tot_u[1]);
       } else {
         double* o = reinterpret_cast<double*>(item.total);
         atomicAdd(o, s_tot_d[0]);
@@ -249,6 +264,9 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
       f1++;
     }
     SB_REQUIRE(f1 > f0, SB_ERR_UNSUPPORTED, "feature %zu has too many bins for shared memory", f0);
+    if (f1 < F && f1 - f0 >= 4) f1 -= (f1 - f0) % 4;  // next tile starts on a multiple of 4
+    SB_REQUIRE(f1 == F || (f1 - f0) % 4 == 0, SB_ERR_UNSUPPORTED,
+               "features %zu.. need more shared memory than one CTA has", f0);
     FeatureTile t;
     t.f0 = (int)f0;
     t.f1 = (int)f1;
@@ -287,6 +305,8 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.ntiles = L.ntiles;
   a.flush_rows = fixed_rows_per_flush(L.quant_bits);
   a.rows_done = L.rows_done;
+  a.pool_mask = L.pool_mask;
+  a.FW = (int)((L.g->F + 31) / 32);
   int grid = hist_grid(ctx, L.g);
   if (L.fixed) SB_LAUNCH(ctx, k_hist<true>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
   else SB_LAUNCH(ctx, k_hist<false>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
@@ -382,6 +402,7 @@ int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m
   L.tiles = d_tiles.p;
   L.ntiles = (int)g->tiles.size();
   L.rows_done = nullptr;
+  L.pool_mask = nullptr;
   if (m) SB_TRY(launch_hist(ctx, L));
   const double2* res = d_hist.p;
   if (L.fixed) {

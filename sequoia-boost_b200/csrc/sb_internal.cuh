@@ -144,6 +144,7 @@ struct HistLaunch {
   const FeatureTile* tiles;  // device
   int ntiles;
   unsigned long long* rows_done;  // device counter of sampled rows, or null
+  const uint32_t* pool_mask;      // device [K][ceil(F/32)]: features to accumulate, or null
 };
 
 int hist_prepare(sb_ctx* ctx, Ghist* g);

@@ -115,3 +115,22 @@ def test_fp32_tree_structure(sb, ctx, orc, variant):
     gaps = om.gaps()
     checked = _compare_structure(m.export()[1], om.export()[1], gaps, 1e-5)
     assert checked > 10
+
+
+@pytest.mark.parametrize("scale", [3e-3, 1e-3])
+def test_near_tie_gains_follow_sequential_rule(sb, ctx, orc, scale):
+    """Small gradients put many candidate gains within 1e-6 of each other, and
+    duplicated columns give exactly equal gains: the device must reproduce
+    consider's sequential `g > best + 1e-6` rule exactly (fixed-point form)."""
+    n = 4000
+    rng = np.random.default_rng(17)
+    base = rng.standard_normal((n, 4)).astype(np.float32)
+    x = np.concatenate([base, base[:, ::-1], np.round(base, 1), base[:, :2]], axis=1)
+    g = np.stack([rng.standard_normal(n) * scale, np.ones(n)], axis=1).astype(np.float32)
+    rows = np.arange(n, dtype=np.uint32)
+    p = sb.TrainingParams(hist_precision="fixed", max_depth=5, min_child_weight=0.0, lambda_=1.0)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    m = sb.HistTreeBuilder(p, ctx=ctx).build(gh, g, rows)
+    gq, _, _ = orc.quantize(g, 16)
+    om = orc.tree_build(orc.data(x), p, gq, rows)
+    assert_trees_equal(m.export(), om.export())
