@@ -368,16 +368,20 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
                                              float missing, const uint32_t* __restrict__ foff,
                                              const float* __restrict__ cuts,
                                              const uint8_t* __restrict__ is_cat,
-                                             uint16_t* __restrict__ bins) {
+                                             const int* __restrict__ fbase,
+                                             const int* __restrict__ fmiss,
+                                             uint16_t* __restrict__ bins,
+                                             uint16_t* __restrict__ bins_col) {
   const bool miss_nan = isnan(missing);
   size_t total = n * (size_t)Fp;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
     size_t r = i / Fp;
     int f = (int)(i - r * Fp);
-    uint16_t out = MISSING_BIN;
+    uint16_t out = MISSING_BIN;  // padding columns
     if (f < F) {
       float v = X[r * F + f];
+      out = (uint16_t)fmiss[f];
       if (!is_missing_d(v, missing, miss_nan)) {
         uint32_t s = foff[f], e = foff[f + 1];
         uint32_t len = e - s;
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
             else if (c > v) hi = mid;
             else { found = mid; break; }
           }
-          out = (uint16_t)found;
+          out = (uint16_t)(fbase[f] + (int)found);
         } else {
           uint32_t lo = 0, hi = len;  // partition_point(c <= v)
           while (lo < hi) {
@@ -398,11 +402,12 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
             if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
           }
           uint32_t local = lo < len - 1 ? lo : len - 1;
-          out = (uint16_t)local;
+          out = (uint16_t)(fbase[f] + (int)local);
         }
       }
     }
     bins[i] = out;
+    if (f < F) bins_col[(size_t)f * n + r] = out;
   }
 }
 
@@ -513,12 +518,17 @@ int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t
   SB_CUDA(cudaMemcpyAsync(g->foff.p, g->h_foff.data(), (F + 1) * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(g->cuts.p, g->h_cuts.data(), g->total_bins * 4, cudaMemcpyHostToDevice, st));
 
+  SB_TRY(hist_prepare(ctx, g));  // feature tiles fix the bin codes
+  SB_TRY(g->fbase.alloc(ctx, F));
+  SB_TRY(g->fmiss.alloc(ctx, F));
+  SB_CUDA(cudaMemcpyAsync(g->fbase.p, g->h_fbase.data(), F * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(g->fmiss.p, g->h_fmiss.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_TRY(g->bins.alloc(ctx, n * g->Fp));
+  SB_TRY(g->bins_col.alloc(ctx, n * F));
   size_t total = n * g->Fp;
   unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 32);
   SB_LAUNCH(ctx, k_bin, blocks, 256, 0, d_X, n, (int)F, (int)g->Fp, missing, g->foff.p, g->cuts.p,
-            g->is_cat.p, g->bins.p);
-  SB_TRY(hist_prepare(ctx, g));
+            g->is_cat.p, g->fbase.p, g->fmiss.p, g->bins.p, g->bins_col.p);
   SB_CUDA(cudaStreamSynchronize(st));  // temporaries are released on return
   return SB_OK;
 }
@@ -584,6 +594,11 @@ int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins) {
   SB_CUDA(cudaMemcpy2DAsync(local_bins, g->F * 2, g->bins.p, g->Fp * 2, g->F * 2, g->n,
                             cudaMemcpyDeviceToHost, g->ctx->stream));
   SB_CUDA(cudaStreamSynchronize(g->ctx->stream));
+  for (size_t r = 0; r < g->n; ++r)  // tile-relative codes -> local bins
+    for (size_t f = 0; f < g->F; ++f) {
+      uint16_t& c = local_bins[r * g->F + f];
+      c = (int)c == g->h_fmiss[f] ? sb::MISSING_BIN : (uint16_t)((int)c - g->h_fbase[f]);
+    }
   return SB_OK;
 }
 

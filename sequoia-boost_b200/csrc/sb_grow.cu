@@ -55,7 +55,10 @@ struct BState {
   int K, F, FW, HB, total_bins, max_depth, maxn, maxw, cat_cap;
   size_t n, Fp;
   // binned data
-  const uint16_t* bins;
+  const uint16_t* bins;      // tile-relative codes, row-major
+  const uint16_t* bins_col;  // the same, feature-major
+  const int* fbase;          // code of local bin 0, per feature
+  const int* fmiss;          // code of a missing entry, per feature
   const uint32_t* foff;
   const float* cuts;
   const uint8_t* is_cat;
@@ -175,10 +178,6 @@ __device__ T block_scan_excl(T v, T* total, T* sm) {
   return r;
 }
 
-__device__ __forceinline__ void atomic_max_f(unsigned int* a, float v) {
-  atomicMax(a, __float_as_uint(fabsf(v)));  // non-negative floats order as integers
-}
-
 __device__ __forceinline__ float sigmoidf_ref(float x) {  // classification.rs:7-15
   if (x >= 0.0f) return __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-x)));
   float e = expf(x);
@@ -255,8 +254,14 @@ __global__ void k_gradient(BState S) {
     if (!S.ext_gpair) S.rows0[r] = (uint32_t)r | (keep ? 0u : UNSAMPLED);
     kept += keep ? 1u : 0u;
   }
+  // one atomic per block and counter (same-address atomics per warp serialise)
+  __shared__ unsigned int s_kept;
+  __shared__ unsigned int s_max[32];
+  if (threadIdx.x == 0) s_kept = 0;
+  if (threadIdx.x < 32) s_max[threadIdx.x] = 0u;
+  __syncthreads();
   for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xFFFFFFFFu, kept, o);
-  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(S.kept, kept);
+  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(&s_kept, kept);
   if (S.fixed) {
     for (int c = 0; c < K && c < 16; ++c) {
       float a = mg[c], b = mh[c];
@@ -265,11 +270,15 @@ __global__ void k_gradient(BState S) {
         b = fmaxf(b, __shfl_xor_sync(0xFFFFFFFFu, b, o));
       }
       if ((threadIdx.x & 31) == 0) {
-        atomic_max_f(&S.maxabs[2 * c], a);
-        atomic_max_f(&S.maxabs[2 * c + 1], b);
+        atomicMax(&s_max[2 * c], __float_as_uint(a));
+        atomicMax(&s_max[2 * c + 1], __float_as_uint(b));
       }
     }
   }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_kept) atomicAdd(S.kept, s_kept);
+  if (S.fixed && threadIdx.x < 2 * K && threadIdx.x < 32 && s_max[threadIdx.x])
+    atomicMax(&S.maxabs[threadIdx.x], s_max[threadIdx.x]);
 }
 
 // Column subset of node `nid` (sampler.rs:52-70 with sb_sampling.h keys),
@@ -418,14 +427,19 @@ __global__ void k_quantize(BState S) {
     eg = fmaxf(eg, fabsf(__fsub_rn(v.x, ldexpf((float)qg, -sg))));
     eh = fmaxf(eh, fabsf(__fsub_rn(v.y, ldexpf((float)qh, -sh))));
   }
+  __shared__ unsigned int s_e[2];
+  if (threadIdx.x < 2) s_e[threadIdx.x] = 0u;
+  __syncthreads();
   for (int o = 16; o > 0; o >>= 1) {
     eg = fmaxf(eg, __shfl_xor_sync(0xFFFFFFFFu, eg, o));
     eh = fmaxf(eh, __shfl_xor_sync(0xFFFFFFFFu, eh, o));
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicMax((unsigned int*)&S.qerr[0], __float_as_uint(eg));
-    atomicMax((unsigned int*)&S.qerr[1], __float_as_uint(eh));
+    atomicMax(&s_e[0], __float_as_uint(eg));
+    atomicMax(&s_e[1], __float_as_uint(eh));
   }
+  __syncthreads();
+  if (threadIdx.x < 2 && s_e[threadIdx.x]) atomicMax((unsigned int*)&S.qerr[0] + threadIdx.x, s_e[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------- K6
@@ -1080,33 +1094,34 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
 }
 
 // K7 + K8: partition every split node's rows into its two children (left rows
-// fill the segment from its start, right rows from its end; order is kept
-// within a tile), and the margin update (train.rs:326-328) for rows whose node
-// is final. Each thread owns 16 consecutive positions of a 4096-row tile, so
-// 16 independent bin loads are in flight per thread; one packed block scan
-// gives every thread its left / right offsets.
+// fill the segment from its start, right rows from its end), and the margin
+// update (train.rs:326-328) for rows whose node is final. A warp walks 32
+// consecutive positions per step (coalesced row-id loads); ballots compact the
+// left / right rows into contiguous runs (coalesced stores); the split
+// feature's codes come from the feature-major copy, read in ascending row
+// order within each run so shallow levels share DRAM sectors.
 constexpr int PART_THREADS = 256;
-constexpr int PART_PER = PART_TILE / PART_THREADS;
+constexpr int PART_WARPS = PART_THREADS / 32;
+constexpr int PART_STEPS = PART_TILE / PART_THREADS;  // 32-row steps per warp
 __global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
-  __shared__ unsigned int sm_u[33];
+  __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
   __shared__ unsigned int s_base[2];
   const bool last = (d + 1 == S.max_depth);
   const int ntiles = *S.ptile_count;
   const uint32_t* rows_cur_all = (d & 1) ? S.rows1 : S.rows0;
   uint32_t* rows_nxt_all = (d & 1) ? S.rows0 : S.rows1;
   const int K = S.K;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tile = S.ptiles[t];
     const int k = tile.x, nid = tile.y;
     const size_t ni = NI(S, k, nid);
     const uint32_t* rows_cur = rows_cur_all + (d == 0 ? 0 : (size_t)k * S.n);
     uint32_t* rows_nxt = rows_nxt_all + (size_t)k * S.n;
-    const int valid = S.split[ni].valid;
-    const int p0 = tile.z + threadIdx.x * PART_PER;
-    const int pe = min(tile.w, p0 + PART_PER);
-    if (!valid) {  // a final leaf: its rows take the leaf value
+    if (!S.split[ni].valid) {  // a final leaf: its rows take the leaf value
       const float lv = S.leafval[ni];
-      for (int p = p0; p < pe; ++p) {
+      for (int p = tile.z + threadIdx.x; p < tile.w; p += PART_THREADS) {
         const uint32_t rv = rows_cur[p];
         const uint32_t id = rv & ~UNSAMPLED;
         if (S.update_margin) S.margin[(size_t)id * K + k] += lv;
@@ -1115,73 +1130,93 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
       continue;
     }
     const NodeSplit& sp = S.split[ni];
-    const int f = sp.feature, sbin = sp.bin, dl = sp.default_left, isc = sp.is_cat;
-    const int left_id = S.out_nodes[((size_t)(*S.round) * K + k) * S.maxn + nid].left;
-    uint32_t rv[PART_PER];
-    uint16_t bv[PART_PER];
+    const int f = sp.feature, dl = sp.default_left, isc = sp.is_cat;
+    const int fb = S.fbase[f], fmc = S.fmiss[f];
+    const int sbin_code = fb + sp.bin;  // numeric: left iff code <= fbase + split bin
+    const uint16_t* col = S.bins_col + (size_t)f * S.n;
+    const int wbeg = tile.z + warp * (PART_STEPS * 32);
+    uint32_t rv[PART_STEPS];
+    unsigned lm[PART_STEPS];
+    unsigned nl = 0, na = 0, nls = 0, nrs = 0;  // lane-uniform warp totals
 #pragma unroll
-    for (int q = 0; q < PART_PER; ++q) rv[q] = (p0 + q < pe) ? rows_cur[p0 + q] : UNSAMPLED;
+    for (int i = 0; i < PART_STEPS; ++i) {
+      const int p = wbeg + i * 32 + lane;
+      const bool valid = p < tile.w;
+      rv[i] = valid ? rows_cur[p] : UNSAMPLED;
+    }
+    int code[PART_STEPS];
 #pragma unroll
-    for (int q = 0; q < PART_PER; ++q)
-      bv[q] = (p0 + q < pe) ? S.bins[(size_t)(rv[q] & ~UNSAMPLED) * S.Fp + f] : (uint16_t)0;
-    unsigned goleft = 0u;  // bit q: position p0+q goes left
-    unsigned nl = 0, nls = 0, nrs = 0;
+    for (int i = 0; i < PART_STEPS; ++i)
+      code[i] = (wbeg + i * 32 + lane < tile.w) ? (int)col[rv[i] & ~UNSAMPLED] : 0;
 #pragma unroll
-    for (int q = 0; q < PART_PER; ++q) {
-      if (p0 + q >= pe) continue;
-      const uint16_t b = bv[q];
+    for (int i = 0; i < PART_STEPS; ++i) {
+      const bool valid = wbeg + i * 32 + lane < tile.w;
+      const int c = code[i];
       bool go;
-      if (b == MISSING_BIN) go = dl != 0;
-      else if (isc) go = (sp.cat_mask[b >> 5] >> (b & 31)) & 1u;
-      else go = (int)b <= sbin;
-      const bool smp = !(rv[q] & UNSAMPLED);
-      goleft |= (go ? 1u : 0u) << q;
-      nl += go ? 1u : 0u;
-      nls += (go && smp) ? 1u : 0u;
-      nrs += (!go && smp) ? 1u : 0u;
+      if (c == fmc) go = dl != 0;
+      else if (isc) {
+        const int b = c - fb;
+        go = (sp.cat_mask[b >> 5] >> (b & 31)) & 1u;
+      } else go = c <= sbin_code;
+      const bool smp = !(rv[i] & UNSAMPLED);
+      lm[i] = __ballot_sync(0xFFFFFFFFu, valid && go);
+      const unsigned vm = __ballot_sync(0xFFFFFFFFu, valid);
+      nl += __popc(lm[i]);
+      na += __popc(vm);
+      nls += __popc(__ballot_sync(0xFFFFFFFFu, valid && go && smp));
+      nrs += __popc(__ballot_sync(0xFFFFFFFFu, valid && !go && smp));
     }
     if (last) {  // children are final leaves: margins only
-      const size_t li = NI(S, k, left_id), ri = li + 1;
-      const float lv = S.leafval[li], rvv = S.leafval[ri];
-      for (int q = 0; q < PART_PER; ++q) {
-        if (p0 + q >= pe) continue;
-        const uint32_t id = rv[q] & ~UNSAMPLED;
-        const bool go = (goleft >> q) & 1u;
+      const int left_id = S.out_nodes[((size_t)(*S.round) * K + k) * S.maxn + nid].left;
+      const size_t li = NI(S, k, left_id);
+      const float lv = S.leafval[li], rvv = S.leafval[li + 1];
+#pragma unroll
+      for (int i = 0; i < PART_STEPS; ++i) {
+        if (wbeg + i * 32 + lane >= tile.w) continue;
+        const uint32_t id = rv[i] & ~UNSAMPLED;
+        const bool go = (lm[i] >> lane) & 1u;
         if (S.update_margin) S.margin[(size_t)id * K + k] += go ? lv : rvv;
-        if (S.row_leaf) S.row_leaf[id] = (rv[q] & UNSAMPLED) ? -1 : (go ? left_id : left_id + 1);
+        if (S.row_leaf) S.row_leaf[id] = (rv[i] & UNSAMPLED) ? -1 : (go ? left_id : left_id + 1);
       }
       continue;
     }
-    const unsigned nhere = (unsigned)max(0, pe - p0);
-    // one scan over (positions, left) packed as 16 + 16 bits (tile <= 4096)
-    unsigned tot;
-    const unsigned pre = block_scan_excl<unsigned>((nhere << 16) | nl, &tot, sm_u);
-    const unsigned loff = pre & 0xFFFFu, aoff = pre >> 16;
-    const unsigned totl = tot & 0xFFFFu, totall = tot >> 16;
-    unsigned ls = nls, rs = nrs;
-    for (int o = 16; o > 0; o >>= 1) {
-      ls += __shfl_xor_sync(0xFFFFFFFFu, ls, o);
-      rs += __shfl_xor_sync(0xFFFFFFFFu, rs, o);
+    if (lane == 0) {
+      s_wl[warp] = nl;
+      s_wa[warp] = na;
     }
     Fill* fl = &S.fill[ni];
-    if ((threadIdx.x & 31) == 0) {
-      if (ls) atomicAdd(&fl->lsamp, ls);
-      if (rs) atomicAdd(&fl->rsamp, rs);
-    }
-    const unsigned totr = totall - totl;
-    if (threadIdx.x == 0) {
-      s_base[0] = atomicAdd(&fl->left, totl);
-      s_base[1] = atomicAdd(&fl->right, totr);
+    if (lane == 0) {
+      if (nls) atomicAdd(&fl->lsamp, nls);
+      if (nrs) atomicAdd(&fl->rsamp, nrs);
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tl = 0, ta = 0;
+      for (int w = 0; w < PART_WARPS; ++w) {
+        tl += s_wl[w];
+        ta += s_wa[w];
+      }
+      s_base[0] = atomicAdd(&fl->left, tl);
+      s_base[1] = atomicAdd(&fl->right, ta - tl) + (ta - tl);  // right rows fill downwards
+    }
+    __syncthreads();
+    unsigned wl = 0, wa = 0;  // rows of earlier warps of this tile
+    for (int w = 0; w < warp; ++w) {
+      wl += s_wl[w];
+      wa += s_wa[w];
+    }
     const uint2 sg = S.seg[ni];
-    unsigned li = sg.x + s_base[0] + loff;
-    unsigned ri = sg.y - s_base[1] - totr + (aoff - loff);
+    unsigned lpos = sg.x + s_base[0] + wl;            // next left slot of this warp
+    unsigned rpos = sg.y - s_base[1] + (wa - wl);     // next right slot of this warp
 #pragma unroll
-    for (int q = 0; q < PART_PER; ++q) {
-      if (p0 + q >= pe) continue;
-      if ((goleft >> q) & 1u) rows_nxt[li++] = rv[q];
-      else rows_nxt[ri++] = rv[q];
+    for (int i = 0; i < PART_STEPS; ++i) {
+      const bool valid = wbeg + i * 32 + lane < tile.w;
+      const unsigned vm = __ballot_sync(0xFFFFFFFFu, valid);
+      const unsigned rm = vm & ~lm[i];
+      if ((lm[i] >> lane) & 1u) rows_nxt[lpos + __popc(lm[i] & lt)] = rv[i];
+      else if (valid) rows_nxt[rpos + __popc(rm & lt)] = rv[i];
+      lpos += __popc(lm[i]);
+      rpos += __popc(rm);
     }
     __syncthreads();
   }
@@ -1567,6 +1602,9 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.n = b->n;
   S.Fp = g->Fp;
   S.bins = g->bins.p;
+  S.bins_col = g->bins_col.p;
+  S.fbase = g->fbase.p;
+  S.fmiss = g->fmiss.p;
   S.foff = g->foff.p;
   S.cuts = g->cuts.p;
   S.is_cat = g->is_cat.p;

@@ -99,7 +99,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     // multiple of 8 bins, so the load is aligned and stays inside the row.
     const int fl0 = 4 * lane;
     const bool lane_on = fl0 < nf;
-    int lbase[4];
     bool fon[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -108,7 +107,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
       bool on = fl < nf;
       if (on && a.pool_mask && !((a.pool_mask[(size_t)item.k * a.FW + (f >> 5)] >> (f & 31)) & 1u)) on = false;
       fon[j] = on;
-      lbase[j] = on ? (int)a.foff[f] - tile.bin0 : 0;
     }
     for (int i = threadIdx.x; i < 2 * nent; i += blockDim.x) sh_g[i] = 0u;
     if (threadIdx.x < 2) {
@@ -165,8 +163,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
         for (int j = 0; j < 4; ++j) {
           if (!fon[j]) continue;
           const uint32_t w = j < 2 ? bv[q].x : bv[q].y;
-          const uint32_t b = (j & 1) ? (w >> 16) : (w & 0xFFFFu);
-          const int idx = (b == MISSING_BIN) ? tile.nbins + fl0 + j : lbase[j] + (int)b;
+          const int idx = (int)((j & 1) ? (w >> 16) : (w & 0xFFFFu));  // the tile-relative code
           if (FIXED) {
             atomicAdd(reinterpret_cast<int*>(sh_g) + idx, (int)vg[q]);
             atomicAdd(sh_h + idx, vh[q]);
@@ -273,9 +270,17 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
     t.bin0 = (int)g->h_foff[f0];
     t.nbins = (int)(g->h_foff[f1] - g->h_foff[f0]);
     maxb = std::max(maxb, (size_t)(t.nbins + (t.f1 - t.f0)) * 8);
+    SB_REQUIRE(t.nbins + (t.f1 - t.f0) < 0xFFFF, SB_ERR_UNSUPPORTED, "histogram tile too large");
     g->tiles.push_back(t);
     f0 = f1;
   }
+  g->h_fbase.assign(F, 0);
+  g->h_fmiss.assign(F, 0);
+  for (const FeatureTile& t : g->tiles)
+    for (int f = t.f0; f < t.f1; ++f) {
+      g->h_fbase[f] = (int)g->h_foff[f] - t.bin0;
+      g->h_fmiss[f] = t.nbins + (f - t.f0);
+    }
   g->hist_smem_bytes = maxb;
   SB_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));
   SB_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));

@@ -107,7 +107,14 @@ struct Ghist {  // sb_ghist
   float missing = NAN;
   int max_feature_bins = 0;
   int has_categorical = 0;
-  DBuf<uint16_t> bins;     // [n][Fp] local bins
+  // [n][Fp] bin codes, tile-relative: code = fbase[f] + local bin, or
+  // fmiss[f] for a missing entry. A code is the entry's index into the
+  // shared-memory partial of the feature's histogram tile.
+  DBuf<uint16_t> bins;
+  DBuf<uint16_t> bins_col; // [F][n] the same codes, feature-major (partition reads)
+  DBuf<int> fbase;         // [F] foff[f] - tile.bin0
+  DBuf<int> fmiss;         // [F] tile.nbins + (f - tile.f0)
+  std::vector<int> h_fbase, h_fmiss;
   DBuf<uint32_t> foff;     // [F+1]
   DBuf<float> cuts;        // [total_bins]
   DBuf<uint8_t> is_cat;    // [F]
