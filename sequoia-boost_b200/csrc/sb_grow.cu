@@ -27,7 +27,7 @@ namespace sb {
 namespace {
 
 constexpr double K_RT_EPS = 1e-6;  // hist.rs:22
-constexpr int PART_TILE = 4096;    // rows per partition tile
+constexpr int PART_TILE = 2048;    // rows per partition tile
 constexpr int EVAL_THREADS = 256;
 
 struct NodeSplit {
@@ -107,6 +107,8 @@ struct BState {
   unsigned int* kept;       // sampled rows this round
   // gradients
   float* margin;            // [n][K]
+  float* delta;             // [n][K] this round's leaf value of each row (pending add)
+  int apply_delta;          // k_gradient first adds delta into margin
   const float* labels;
   const float* weights;
   float2* gpair;            // [K][n]
@@ -197,6 +199,8 @@ __global__ void k_gradient(BState S) {
     if (!S.ext_gpair) {
       const float w0 = S.weights ? S.weights[r] : 1.0f;
       const float y = S.labels[r];
+      if (S.apply_delta)  // the previous tree's leaf values (train.rs:326-328)
+        for (int c = 0; c < K; ++c) S.margin[r * K + c] = __fadd_rn(S.margin[r * K + c], S.delta[r * K + c]);
       if (K == 1) {
         const float m = S.margin[r];
         float g, h;
@@ -962,6 +966,8 @@ __device__ sb_node make_leaf(float value, float sum_hess) {  // Node::leaf, regt
 __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tiles) {
   __shared__ int sm_i[33];
   __shared__ int s_tile_carry;
+  __shared__ int s_toff[1024], s_nid[1024];
+  __shared__ uint2 s_seg[1024];
   const unsigned long long round = *S.round;
   const int tid = threadIdx.x;
   if (tid == 0) s_tile_carry = 0;
@@ -1063,15 +1069,29 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
           S.leafval[ni] = lv;
         }
       }
-      // partition tiles of this frontier node
+      // partition tiles of this chunk's frontier nodes: one thread per tile,
+      // its node found by a binary search over the chunk's tile offsets
       int tot_t;
-      const int toff = s_tile_carry + block_scan_excl<int>(tiles, &tot_t, sm_i);
-      if (write_tiles && act) {
-        const uint2 sg = S.seg[ni];
-        for (int q = 0; q < tiles && toff + q < S.ptile_cap; ++q) {
-          unsigned b = sg.x + q * PART_TILE;
-          unsigned e = min(sg.y, b + PART_TILE);
-          S.ptiles[toff + q] = make_int4(k, nid, (int)b, (int)e);
+      const int toff = block_scan_excl<int>(tiles, &tot_t, sm_i);
+      if (write_tiles) {
+        s_toff[tid] = toff + tiles;  // inclusive end
+        if (act) {
+          s_seg[tid] = S.seg[ni];
+          s_nid[tid] = nid;
+        }
+        __syncthreads();
+        const int nact = min(cnt - c0, (int)blockDim.x);
+        for (int q = tid; q < tot_t; q += blockDim.x) {
+          int lo = 0, hi = nact - 1;  // first node whose end exceeds q
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_toff[mid] > q) hi = mid; else lo = mid + 1;
+          }
+          const int qi = q - (s_toff[lo] - (int)((s_seg[lo].y - s_seg[lo].x + PART_TILE - 1) / PART_TILE));
+          const unsigned b = s_seg[lo].x + (unsigned)qi * PART_TILE;
+          const unsigned e = min(s_seg[lo].y, b + PART_TILE);
+          const int slot_t = s_tile_carry + q;
+          if (slot_t < S.ptile_cap) S.ptiles[slot_t] = make_int4(k, s_nid[lo], (int)b, (int)e);
         }
       }
       __syncthreads();
@@ -1103,8 +1123,9 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
 constexpr int PART_THREADS = 256;
 constexpr int PART_WARPS = PART_THREADS / 32;
 constexpr int PART_STEPS = PART_TILE / PART_THREADS;  // 32-row steps per warp
-__global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
+__global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) {
   __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
+  __shared__ uint2 s_ws[PART_WARPS];
   __shared__ unsigned int s_base[2];
   const bool last = (d + 1 == S.max_depth);
   const int ntiles = *S.ptile_count;
@@ -1124,7 +1145,7 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
       for (int p = tile.z + threadIdx.x; p < tile.w; p += PART_THREADS) {
         const uint32_t rv = rows_cur[p];
         const uint32_t id = rv & ~UNSAMPLED;
-        if (S.update_margin) S.margin[(size_t)id * K + k] += lv;
+        if (S.update_margin) S.delta[(size_t)id * K + k] = lv;
         if (S.row_leaf) S.row_leaf[id] = (rv & UNSAMPLED) ? -1 : nid;
       }
       continue;
@@ -1175,7 +1196,7 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
         if (wbeg + i * 32 + lane >= tile.w) continue;
         const uint32_t id = rv[i] & ~UNSAMPLED;
         const bool go = (lm[i] >> lane) & 1u;
-        if (S.update_margin) S.margin[(size_t)id * K + k] += go ? lv : rvv;
+        if (S.update_margin) S.delta[(size_t)id * K + k] = go ? lv : rvv;
         if (S.row_leaf) S.row_leaf[id] = (rv[i] & UNSAMPLED) ? -1 : (go ? left_id : left_id + 1);
       }
       continue;
@@ -1183,19 +1204,20 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(BState S, int d) {
     if (lane == 0) {
       s_wl[warp] = nl;
       s_wa[warp] = na;
+      s_ws[warp] = make_uint2(nls, nrs);
     }
     Fill* fl = &S.fill[ni];
-    if (lane == 0) {
-      if (nls) atomicAdd(&fl->lsamp, nls);
-      if (nrs) atomicAdd(&fl->rsamp, nrs);
-    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned tl = 0, ta = 0;
+    if (threadIdx.x == 0) {  // one set of counter atomics per tile
+      unsigned tl = 0, ta = 0, tls = 0, trs = 0;
       for (int w = 0; w < PART_WARPS; ++w) {
         tl += s_wl[w];
         ta += s_wa[w];
+        tls += s_ws[w].x;
+        trs += s_ws[w].y;
       }
+      if (tls) atomicAdd(&fl->lsamp, tls);
+      if (trs) atomicAdd(&fl->rsamp, trs);
       s_base[0] = atomicAdd(&fl->left, tl);
       s_base[1] = atomicAdd(&fl->right, ta - tl) + (ta - tl);  // right rows fill downwards
     }
@@ -1301,6 +1323,12 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
   }
 }
 
+// margin += the last tree's leaf values, when no further round folds them in
+__global__ void k_apply_delta(float* __restrict__ margin, const float* __restrict__ delta, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    margin[i] = __fadd_rn(margin[i], delta[i]);
+}
+
 __global__ void k_round_end(BState S) {
   const unsigned long long round = *S.round;
   for (int k = threadIdx.x; k < S.K; k += blockDim.x) {
@@ -1361,6 +1389,8 @@ struct sb_booster {
   sb::DBuf<uint32_t> d_rows0, d_rows1;
   sb::DBuf<unsigned int> d_kept;
   sb::DBuf<float> d_margin, d_labels, d_weights;
+  sb::DBuf<float> d_delta;   // [n][K] leaf values of the last tree, not yet in d_margin
+  mutable bool delta_pending = false;  // margins are read through const handles
   sb::DBuf<float2> d_gpair;
   sb::DBuf<unsigned long long> d_gpk;
   sb::DBuf<unsigned int> d_maxabs;
@@ -1550,6 +1580,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   SB_TRY(b->d_kept.alloc(ctx, 1));
   SB_CUDA(cudaMemsetAsync(b->d_kept.p, 0, 4, st));
   SB_TRY(b->d_margin.alloc(ctx, b->n * K));
+  SB_TRY(b->d_delta.alloc(ctx, b->n * K));
   SB_TRY(b->d_gpair.alloc(ctx, (size_t)K * b->n));
   const bool fixed = p->hist_precision == SB_HIST_FIXED;
   if (fixed) SB_TRY(b->d_gpk.alloc(ctx, (size_t)K * b->n));
@@ -1652,6 +1683,8 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.rows1 = b->d_rows1.p;
   S.kept = b->d_kept.p;
   S.margin = b->d_margin.p;
+  S.delta = b->d_delta.p;
+  S.apply_delta = 0;
   S.labels = b->d_labels.p;
   S.weights = b->d_weights.p;
   S.gpair = b->d_gpair.p;
@@ -1701,12 +1734,16 @@ int booster_round(sb_booster* b) {
     SB_CUDA(cudaEventRecord(r0, ctx->stream));
   }
   const unsigned gblocks = (unsigned)std::min<size_t>((b->n + 255) / 256, (size_t)ctx->num_sms * 16);
+  S.apply_delta = b->delta_pending ? 1 : 0;
   SB_LAUNCH(ctx, k_gradient, gblocks, 256, 0, S);
+  S.apply_delta = 0;
+  b->delta_pending = S.update_margin != 0;
   SB_LAUNCH(ctx, k_round_prep, (unsigned)b->K, PREP_THREADS, 0, S);
   if (S.fixed) SB_LAUNCH(ctx, k_quantize, gblocks, 256, 0, S);
   HistLaunch L;
   L.g = b->g;
   L.gpair = S.fixed ? (const void*)S.gpk : (const void*)S.gpair;
+  L.gpair_bytes = (size_t)b->K * b->n * 8;
   L.fixed = S.fixed;
   L.quant_bits = S.bits;
   L.items = S.items;
@@ -1827,6 +1864,17 @@ int booster_export(const sb_booster* b, sb_model* m) {
   return SB_OK;
 }
 
+// Folds a pending tree's leaf values into the margins before the host reads them.
+int booster_flush_delta(const sb_booster* b) {
+  if (!b->delta_pending) return SB_OK;
+  sb_ctx* ctx = b->ctx;
+  const size_t nk = b->n * (size_t)b->K;
+  const unsigned blocks = (unsigned)std::min<size_t>((nk + 255) / 256, (size_t)ctx->num_sms * 16);
+  SB_LAUNCH(ctx, k_apply_delta, blocks, 256, 0, b->d_margin.p, b->d_delta.p, nk);
+  b->delta_pending = false;
+  return SB_OK;
+}
+
 int booster_run(sb_booster* b, int n_rounds) {
   SB_TRY(booster_alloc_trees(b, (b->rounds_done + n_rounds) * b->K));
   SB_TRY(booster_set_eval_smem(b));
@@ -1924,6 +1972,7 @@ int sb_booster_update(sb_booster* b, int n_rounds) {
 
 int sb_booster_margins(const sb_booster* b, float* out) {
   SB_REQUIRE(b && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_TRY(sb::booster_flush_delta(b));
   SB_CUDA(cudaMemcpyAsync(out, b->d_margin.p, b->d_margin.bytes(), cudaMemcpyDeviceToHost, b->ctx->stream));
   SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
   return SB_OK;

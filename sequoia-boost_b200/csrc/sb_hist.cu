@@ -25,7 +25,7 @@
 namespace sb {
 namespace {
 
-constexpr int HIST_THREADS = 768;
+constexpr int HIST_THREADS = 1024;
 constexpr int MAX_TILE_FEATURES = 128;  // 4 features per lane
 constexpr int ROWS_PER_WARP = 8;        // rows in flight per warp
 
@@ -36,6 +36,7 @@ struct HistDev {
   size_t n;              // gradient column stride
   int total_bins;
   const void* gpair;
+  size_t gpair_bytes;
   const HistItem* items;
   const uint64_t* prefix;
   const int* count;
@@ -46,6 +47,22 @@ struct HistDev {
   const uint32_t* pool_mask;      // [K][FW] features to accumulate (or null: all)
   int FW;
 };
+
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16).
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// L2 prefetch of row `id`'s codes in the tile and of its gradient pair (the
+// aligned 16 bytes holding it, when they lie inside the gradient array).
+__device__ __forceinline__ void prefetch_row(const HistDev& a, const char* bins_bytes, size_t row_bytes,
+                                             uint32_t pf_bytes, size_t gcol, uint32_t id) {
+  prefetch_l2_bulk(bins_bytes + (size_t)id * row_bytes, pf_bytes);
+  const size_t gb = (gcol + id) * 8;
+  const uintptr_t ga = (reinterpret_cast<uintptr_t>(a.gpair) + gb) & ~uintptr_t(15);
+  if (ga + 16 <= reinterpret_cast<uintptr_t>(a.gpair) + a.gpair_bytes)
+    prefetch_l2_bulk(reinterpret_cast<const void*>(ga), 16);
+}
 
 __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
   int lo = 0, hi = count;  // last i with prefix[i] <= pos
@@ -115,67 +132,90 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     }
     __syncthreads();
 
+    // Lane q < ROWS_PER_WARP holds row q of the warp's batch: its row id and
+    // its gradient pair; the other lanes get them by shuffles. Every lane then
+    // loads its 4 codes of each row. Row ids are loaded two batches ahead, and
+    // the next batch's bin rows and gradient pairs are prefetched into L2 with
+    // bulk prefetches (no registers held), so the current batch's loads hit L2.
     double tg = 0.0, th = 0.0;
     long long tqg = 0;
     unsigned long long tqh = 0;
     unsigned int nsampled = 0;
     const size_t gcol = (size_t)item.k * a.n;
     const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
-    for (uint32_t p = pbeg + warp * ROWS_PER_WARP; p < pend; p += nwarps * ROWS_PER_WARP) {
-      uint32_t rid[ROWS_PER_WARP];
-#pragma unroll
-      for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const uint32_t pp = p + q;
-        rid[q] = pp < pend ? item.rows[pp] : UNSAMPLED;
+    const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
+    // the tile's part of a row, widened to 16-byte boundaries (rows are
+    // 16-byte aligned: Fp is a multiple of 8 bins)
+    const uint32_t pf_lo = (uint32_t)(tile.f0 * 2) & ~15u;
+    const uint32_t pf_bytes = (((uint32_t)(tile.f1 * 2) + 15u) & ~15u) - pf_lo;
+    const char* bins_bytes = reinterpret_cast<const char*>(a.bins) + pf_lo;
+    const size_t row_bytes = a.Fp * sizeof(uint16_t);
+    uint32_t p = pbeg + warp * ROWS_PER_WARP;
+    uint32_t next_rid = UNSAMPLED, next2_rid = UNSAMPLED;
+    if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
+    if (lane < ROWS_PER_WARP && p + stride + lane < pend) next2_rid = item.rows[p + stride + lane];
+    if (lane < ROWS_PER_WARP && !(next_rid & UNSAMPLED)) prefetch_row(a, bins_bytes, row_bytes, pf_bytes, gcol, next_rid);
+    for (; p < pend; p += stride) {
+      const uint32_t my_rid = next_rid;
+      next_rid = next2_rid;
+      const uint32_t pn = p + 2 * stride + lane;
+      next2_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
+      if (lane < ROWS_PER_WARP && !(next_rid & UNSAMPLED))  // the next batch, into L2
+        prefetch_row(a, bins_bytes, row_bytes, pf_bytes, gcol, next_rid);
+      const bool my_use = lane < ROWS_PER_WARP && !(my_rid & UNSAMPLED);
+      uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
+      if (my_use) {
+        if (FIXED) {
+          const unsigned long long pk =
+              reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          my_g = (uint32_t)(pk >> 32);
+          my_h = (uint32_t)(pk & 0xFFFFFFFFull);
+        } else {
+          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          my_g = __float_as_uint(v.x);
+          my_h = __float_as_uint(v.y);
+        }
+        nsampled++;
+        if (want_total) {
+          if (FIXED) {
+            tqg += (int)my_g;
+            tqh += my_h;
+          } else {
+            tg += (double)__uint_as_float(my_g);
+            th += (double)__uint_as_float(my_h);
+          }
+        }
       }
-      uint32_t vg[ROWS_PER_WARP], vh[ROWS_PER_WARP];  // FIXED ints or FP32 float bits
+      const unsigned use_mask = __ballot_sync(0xFFFFFFFFu, my_use);
       uint2 bv[ROWS_PER_WARP];
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const bool use = !(rid[q] & UNSAMPLED);
-        const size_t id = rid[q] & ~UNSAMPLED;
-        if (FIXED) {
-          const unsigned long long pk = use ? reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + id] : 0ull;
-          vg[q] = (uint32_t)(pk >> 32);
-          vh[q] = (uint32_t)(pk & 0xFFFFFFFFull);
-        } else {
-          const float2 v = use ? reinterpret_cast<const float2*>(a.gpair)[gcol + id] : make_float2(0.f, 0.f);
-          vg[q] = __float_as_uint(v.x);
-          vh[q] = __float_as_uint(v.y);
-        }
-        bv[q] = (use && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
-                                 : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q) & ~UNSAMPLED;
+        bv[q] = (((use_mask >> q) & 1u) && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
+                                                    : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
       }
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        if (rid[q] & UNSAMPLED) continue;
-        nsampled++;
-        if (want_total && lane == 0) {
-          if (FIXED) {
-            tqg += (int)vg[q];
-            tqh += vh[q];
-          } else {
-            tg += (double)__uint_as_float(vg[q]);
-            th += (double)__uint_as_float(vh[q]);
-          }
-        }
+        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, my_g, q);
+        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, my_h, q);
+        if (!((use_mask >> q) & 1u)) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           if (!fon[j]) continue;
           const uint32_t w = j < 2 ? bv[q].x : bv[q].y;
           const int idx = (int)((j & 1) ? (w >> 16) : (w & 0xFFFFu));  // the tile-relative code
           if (FIXED) {
-            atomicAdd(reinterpret_cast<int*>(sh_g) + idx, (int)vg[q]);
-            atomicAdd(sh_h + idx, vh[q]);
+            atomicAdd(reinterpret_cast<int*>(sh_g) + idx, (int)vg);
+            atomicAdd(sh_h + idx, vh);
           } else {
-            atomicAdd(reinterpret_cast<float*>(sh_g) + idx, __uint_as_float(vg[q]));
-            atomicAdd(reinterpret_cast<float*>(sh_h) + idx, __uint_as_float(vh[q]));
+            atomicAdd(reinterpret_cast<float*>(sh_g) + idx, __uint_as_float(vg));
+            atomicAdd(reinterpret_cast<float*>(sh_h) + idx, __uint_as_float(vh));
           }
         }
       }
     }
-    if (a.rows_done && lane == 0 && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
-    if (want_total && lane == 0) {
+    if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
+    if (want_total && lane < ROWS_PER_WARP) {
       if (FIXED) {
         atomicAdd(&s_tot_u[0], (unsigned long long)tqg);
         atomicAdd(&s_tot_u[1], tqh);
@@ -303,6 +343,7 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.n = L.g->n;
   a.total_bins = (int)L.g->total_bins;
   a.gpair = L.gpair;
+  a.gpair_bytes = L.gpair_bytes;
   a.items = L.items;
   a.prefix = L.prefix;
   a.count = L.count;
@@ -398,6 +439,7 @@ int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m
   HistLaunch L;
   L.g = g;
   L.gpair = gsrc;
+  L.gpair_bytes = n * 8;
   L.fixed = precision == SB_HIST_FIXED;
   L.quant_bits = bits;
   L.items = d_item.p;
