@@ -199,6 +199,27 @@ int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m
 int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats* child,
                      sb_gradstats* out, size_t total_bins);
 
+/* No counterpart in the reference. The FP32 form of sb_hist_build for callers
+ * that cannot let a library allocate device memory, such as a process that
+ * hands all free HBM to its own pool allocator at start-up, where any later
+ * allocation by a library can fail at an arbitrary time. Inputs and output are
+ * the caller's DEVICE buffers: d_rows[m] (row ids below n), d_gpair[n] and
+ * d_out[total_bins] (overwritten), on the context's device.
+ * Working memory is one static device array of SB_STATIC_SCRATCH_BYTES
+ * (8 MiB). The node histogram in it takes 16 bytes per bin plus one missing
+ * bin per feature, so total_bins + n_cols must stay below about 524,000;
+ * a larger index is rejected with SB_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array, and the call clears the histogram
+ * part itself: calls that overlap in time (from other threads, or other
+ * contexts on the same device) race and must be serialised by the caller.
+ * Returns after d_out is written. */
+#define SB_STATIC_SCRATCH_BYTES (8u << 20)
+int sb_hist_build_static(sb_ctx* ctx, const sb_ghist* g, const uint32_t* d_rows, size_t m,
+                         const sb_gradpair* d_gpair, size_t n, sb_gradstats* d_out,
+                         size_t total_bins);
+
 /* ---------------------------------------------------- tree / boosting loop */
 typedef struct sb_model sb_model;
 typedef struct sb_booster sb_booster;

@@ -150,6 +150,7 @@ SIGNATURES = {
                             ctypes.POINTER(SbGradStats), SZ]),
     "sb_hist_subtract": (I32, [P, ctypes.POINTER(SbGradStats), ctypes.POINTER(SbGradStats),
                                ctypes.POINTER(SbGradStats), SZ]),
+    "sb_hist_build_static": (I32, [P, P, P, SZ, P, SZ, P, SZ]),  # device pointers
     "sb_tree_build": (I32, [P, P, ctypes.POINTER(SbTrainParams), ctypes.POINTER(SbGradPair), SZ,
                             U32P, SZ, ctypes.c_uint64, ctypes.c_uint32, I32P, ctypes.POINTER(P)]),
     "sb_booster_create": (I32, [P, P, ctypes.POINTER(SbTrainParams), F32P, F32P, F32P,

@@ -1,0 +1,76 @@
+"""sb_hist_build_static (the histogram build that allocates no device memory)
+against sb_hist_build on the same inputs. Collected after every other test
+file, so it also runs after the rest of the suite has used the device."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from gpu_helpers import mixed_data, random_gpair
+
+pytestmark = pytest.mark.gpu
+
+
+def _static_build(sb, ctx, gh, d_rows, m, d_gpair, n, d_out, total):
+    lib = sb._abi.lib()
+    return lib.sb_hist_build_static(ctx.h, gh.h, ctypes.c_void_p(d_rows), m, ctypes.c_void_p(d_gpair), n,
+                                    ctypes.c_void_p(d_out), total)
+
+
+def test_static_scratch_build_matches_sb_hist_build_twice(sb, ctx):
+    import torch
+    n, f = 60000, 24
+    x, _ = mixed_data(n, f, seed=11)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    total = gh.total_bins
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda", 0)
+    # two calls in a row with different rows and gradients: the second must not
+    # see anything the first left in the shared scratch
+    for call, frac in enumerate((0.6, 0.35)):
+        g = random_gpair(n, seed=20 + call, logistic=True)
+        rows = np.sort(rng.choice(n, int(n * frac), replace=False)).astype(np.uint32)
+        want = sb.GpuBackend("fp32", ctx=ctx).build(gh, rows, g)
+        d_rows = torch.from_numpy(rows.astype(np.int32)).to(dev)
+        d_g = torch.from_numpy(np.ascontiguousarray(g, np.float32)).to(dev)
+        d_out = torch.full((total, 2), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        rc = _static_build(sb, ctx, gh, d_rows.data_ptr(), rows.size, d_g.data_ptr(), n, d_out.data_ptr(),
+                           total)
+        assert rc == 0, sb._abi.lib().sb_last_error()
+        got = d_out.cpu().numpy()
+        # both are FP32 shared-memory partials summed into f64 with atomics in
+        # a different order: equal within 1e-5 of each bin's absolute mass
+        mag = sb.GpuBackend("fp32", ctx=ctx).build(gh, rows, np.abs(g))
+        err = np.abs(got - want)
+        assert np.all(err <= 1e-5 * mag + 1e-12), (call, float(np.max(err / (mag + 1e-30))))
+
+
+def test_static_scratch_rejects_bad_rows_and_large_indexes(sb, ctx):
+    import torch
+    dev = torch.device("cuda", 0)
+    n, f = 2000, 6
+    x, _ = mixed_data(n, f, seed=3)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    total = gh.total_bins
+    d_g = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    d_out = torch.zeros((total, 2), dtype=torch.float64, device=dev)
+    d_rows = torch.tensor([0, 5, n], dtype=torch.int32, device=dev)  # one id out of range
+    torch.cuda.synchronize()
+    rc = _static_build(sb, ctx, gh, d_rows.data_ptr(), 3, d_g.data_ptr(), n, d_out.data_ptr(), total)
+    assert rc == sb._abi.SB_ERR_INVALID_ARG
+    assert b"not below n_rows" in sb._abi.lib().sb_last_error()
+
+    # 2100 features of 257 bins: about 541,800 histogram bins, above the scratch limit
+    rng = np.random.default_rng(1)
+    big = rng.normal(size=(300, 2100)).astype(np.float32)
+    gb = sb.GHistIndex(sb.DMatrix(big), ctx=ctx)
+    tb = gb.total_bins
+    assert tb + 2100 > (8 << 20) // 16
+    d_gb = torch.zeros((300, 2), dtype=torch.float32, device=dev)
+    d_ob = torch.zeros((tb, 2), dtype=torch.float64, device=dev)
+    d_rb = torch.arange(300, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    rc = _static_build(sb, ctx, gb, d_rb.data_ptr(), 300, d_gb.data_ptr(), 300, d_ob.data_ptr(), tb)
+    assert rc == sb._abi.SB_ERR_UNSUPPORTED
+    assert b"SB_STATIC_SCRATCH_BYTES" in sb._abi.lib().sb_last_error()
