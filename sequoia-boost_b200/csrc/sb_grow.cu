@@ -885,26 +885,32 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
     cf = fstar;
     cidx = R[fstar].def_idx;
   }
-  // ambiguous records after the winner, in candidate order (lane-uniform walk)
-  for (int f = fstar < 0 ? 0 : fstar; f < S.F; ++f) {
-    if (!in_mask(fm, f) || !(M[f] > K_RT_EPS)) continue;
-    const FeatRec& r = R[f];
-    if (r.namb == 0) continue;
-    if (r.namb > AMB_MAX) {  // overflow: exact replay of this feature from b
-      Chosen c = scan_feature<SCAN_REPLAY>(S, H, k, f, E, b, cs, s_gains[warp], nullptr);
-      if (c.cand >= 0) {
-        b = c.gain;
-        cf = f;
-        cidx = c.cand;
+  // ambiguous records after the winner, in candidate order: 32 features are
+  // tested at a time, and the (rare) features holding any are walked in order
+  for (int f0 = fstar < 0 ? 0 : fstar; f0 < S.F; f0 += 32) {
+    const int fl = f0 + lane;
+    const bool has = fl < S.F && in_mask(fm, fl) && M[fl] > K_RT_EPS && R[fl].namb > 0;
+    unsigned hm = __ballot_sync(0xFFFFFFFFu, has);
+    while (hm) {
+      const int f = f0 + __ffs(hm) - 1;
+      hm &= hm - 1;
+      const FeatRec& r = R[f];
+      if (r.namb > AMB_MAX) {  // overflow: exact replay of this feature from b
+        Chosen c = scan_feature<SCAN_REPLAY>(S, H, k, f, E, b, cs, s_gains[warp], nullptr);
+        if (c.cand >= 0) {
+          b = c.gain;
+          cf = f;
+          cidx = c.cand;
+        }
+        continue;
       }
-      continue;
+      for (int a = 0; a < r.namb; ++a)
+        if (r.amb_gain[a] > b + K_RT_EPS) {
+          b = r.amb_gain[a];
+          cf = f;
+          cidx = r.amb_idx[a];
+        }
     }
-    for (int a = 0; a < r.namb; ++a)
-      if (r.amb_gain[a] > b + K_RT_EPS) {
-        b = r.amb_gain[a];
-        cf = f;
-        cidx = r.amb_idx[a];
-      }
   }
   if (lane == 0) {
     best->feature = -1;
@@ -1743,7 +1749,6 @@ int booster_round(sb_booster* b) {
   HistLaunch L;
   L.g = b->g;
   L.gpair = S.fixed ? (const void*)S.gpk : (const void*)S.gpair;
-  L.gpair_bytes = (size_t)b->K * b->n * 8;
   L.fixed = S.fixed;
   L.quant_bits = S.bits;
   L.items = S.items;

@@ -36,7 +36,6 @@ struct HistDev {
   size_t n;              // gradient column stride
   int total_bins;
   const void* gpair;
-  size_t gpair_bytes;
   const HistItem* items;
   const uint64_t* prefix;
   const int* count;
@@ -47,22 +46,6 @@ struct HistDev {
   const uint32_t* pool_mask;      // [K][FW] features to accumulate (or null: all)
   int FW;
 };
-
-// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16).
-__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// L2 prefetch of row `id`'s codes in the tile and of its gradient pair (the
-// aligned 16 bytes holding it, when they lie inside the gradient array).
-__device__ __forceinline__ void prefetch_row(const HistDev& a, const char* bins_bytes, size_t row_bytes,
-                                             uint32_t pf_bytes, size_t gcol, uint32_t id) {
-  prefetch_l2_bulk(bins_bytes + (size_t)id * row_bytes, pf_bytes);
-  const size_t gb = (gcol + id) * 8;
-  const uintptr_t ga = (reinterpret_cast<uintptr_t>(a.gpair) + gb) & ~uintptr_t(15);
-  if (ga + 16 <= reinterpret_cast<uintptr_t>(a.gpair) + a.gpair_bytes)
-    prefetch_l2_bulk(reinterpret_cast<const void*>(ga), 16);
-}
 
 __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
   int lo = 0, hi = count;  // last i with prefix[i] <= pos
@@ -132,11 +115,9 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     }
     __syncthreads();
 
-    // Lane q < ROWS_PER_WARP holds row q of the warp's batch: its row id and
-    // its gradient pair; the other lanes get them by shuffles. Every lane then
-    // loads its 4 codes of each row. Row ids are loaded two batches ahead, and
-    // the next batch's bin rows and gradient pairs are prefetched into L2 with
-    // bulk prefetches (no registers held), so the current batch's loads hit L2.
+    // Lane q < ROWS_PER_WARP holds row q of the warp's batch: its row id
+    // (loaded one batch ahead) and its gradient pair; the other lanes get them
+    // by shuffles. Every lane then loads its 4 codes of each row.
     double tg = 0.0, th = 0.0;
     long long tqg = 0;
     unsigned long long tqh = 0;
@@ -144,24 +125,13 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     const size_t gcol = (size_t)item.k * a.n;
     const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
     const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
-    // the tile's part of a row, widened to 16-byte boundaries (rows are
-    // 16-byte aligned: Fp is a multiple of 8 bins)
-    const uint32_t pf_lo = (uint32_t)(tile.f0 * 2) & ~15u;
-    const uint32_t pf_bytes = (((uint32_t)(tile.f1 * 2) + 15u) & ~15u) - pf_lo;
-    const char* bins_bytes = reinterpret_cast<const char*>(a.bins) + pf_lo;
-    const size_t row_bytes = a.Fp * sizeof(uint16_t);
     uint32_t p = pbeg + warp * ROWS_PER_WARP;
-    uint32_t next_rid = UNSAMPLED, next2_rid = UNSAMPLED;
+    uint32_t next_rid = UNSAMPLED;
     if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
-    if (lane < ROWS_PER_WARP && p + stride + lane < pend) next2_rid = item.rows[p + stride + lane];
-    if (lane < ROWS_PER_WARP && !(next_rid & UNSAMPLED)) prefetch_row(a, bins_bytes, row_bytes, pf_bytes, gcol, next_rid);
     for (; p < pend; p += stride) {
       const uint32_t my_rid = next_rid;
-      next_rid = next2_rid;
-      const uint32_t pn = p + 2 * stride + lane;
-      next2_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
-      if (lane < ROWS_PER_WARP && !(next_rid & UNSAMPLED))  // the next batch, into L2
-        prefetch_row(a, bins_bytes, row_bytes, pf_bytes, gcol, next_rid);
+      const uint32_t pn = p + stride + lane;
+      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
       const bool my_use = lane < ROWS_PER_WARP && !(my_rid & UNSAMPLED);
       uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
       if (my_use) {
@@ -343,7 +313,6 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.n = L.g->n;
   a.total_bins = (int)L.g->total_bins;
   a.gpair = L.gpair;
-  a.gpair_bytes = L.gpair_bytes;
   a.items = L.items;
   a.prefix = L.prefix;
   a.count = L.count;
@@ -439,7 +408,6 @@ int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m
   HistLaunch L;
   L.g = g;
   L.gpair = gsrc;
-  L.gpair_bytes = n * 8;
   L.fixed = precision == SB_HIST_FIXED;
   L.quant_bits = bits;
   L.items = d_item.p;

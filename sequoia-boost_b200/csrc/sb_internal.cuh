@@ -142,7 +142,6 @@ struct HistItem {
 struct HistLaunch {
   const Ghist* g;
   const void* gpair;     // FP32: float2 [K][n]; FIXED: uint64 packed [K][n]
-  size_t gpair_bytes = 0;  // bytes readable from gpair (bounds its L2 prefetches; 0 = none)
   int fixed;
   int quant_bits;
   const HistItem* items; // device

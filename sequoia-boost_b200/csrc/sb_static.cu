@@ -124,7 +124,6 @@ int sb_hist_build_static(sb_ctx* ctx, const sb_ghist* g, const uint32_t* d_rows,
     HistLaunch L;
     L.g = g;
     L.gpair = d_gpair;
-    L.gpair_bytes = n * 8;
     L.fixed = 0;
     L.quant_bits = 16;
     L.items = d_item;
