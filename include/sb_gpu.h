@@ -265,6 +265,11 @@ typedef struct sb_booster_stats {
   int32_t quant_shift_grad;    /* last round's power-of-two scale exponents */
   int32_t quant_shift_hess;
 } sb_booster_stats;
+/* No counterpart in the reference (an engine option). Rounds after the
+ * second are recorded once as a CUDA graph and replayed with one launch each
+ * (re-recorded when the booster's buffers change); 0 launches every kernel
+ * separately. On by default. */
+int sb_booster_set_graphs(sb_booster* b, int enable);
 /* timing != 0 brackets every histogram launch with CUDA events (adds a
  * little overhead); stats accumulate until reset. */
 int sb_booster_set_timing(sb_booster* b, int timing);
@@ -308,6 +313,41 @@ int sb_predict(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float 
  * [n][K][n_cols+1], bias last. */
 int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
                         float missing, float* out);
+
+/* -------------------------------------------------------- serving loop */
+/* No counterpart in the reference (it predicts one call at a time). A tree
+ * ensemble kept resident in HBM answers margin requests (the output of
+ * sb_predict_margin with ntree_limit 0 and no base_margin, [n][K]) and
+ * TreeSHAP requests (the output of sb_predict_contribs, [n][K][n_cols+1])
+ * from any number of threads, with continuous batching: a dispatcher thread
+ * joins runs of queued requests of one kind into device batches, admits a
+ * batch when its buffers fit in the free part of the loop's memory budget,
+ * and keeps up to n_slots batches in flight on their own streams (margins at
+ * high stream priority, TreeSHAP at low). Host buffers may be pageable;
+ * page-locked X and out make the copies asynchronous. */
+typedef struct sb_server sb_server;
+enum { SB_REQ_MARGIN = 0, SB_REQ_CONTRIBS = 1 };
+typedef struct sb_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t batches, rows;        /* device batches launched and their rows */
+  uint64_t max_batch_requests;   /* most requests joined into one batch */
+  uint64_t memory_waits;         /* times the queue head waited for memory */
+  uint64_t mem_bytes, mem_peak;  /* budget and the most of it in use */
+} sb_server_stats;
+/* mem_bytes: device memory for request buffers (0 = half of what is free
+ * now); n_slots: batches in flight (1..64). The model must outlive the loop. */
+int sb_server_create(sb_ctx* ctx, sb_model* m, size_t mem_bytes, int n_slots, sb_server** out);
+/* Queues a request; X [n_rows][n_cols] and out stay owned by the caller and
+ * must stay valid until sb_server_wait returns for the ticket. */
+int sb_server_submit(sb_server* s, int kind, const float* X, size_t n_rows, size_t n_cols,
+                     float missing, float* out, uint64_t* ticket);
+/* Blocks until the request is done (timeout_ms < 0: no limit); returns its
+ * status (SB_ERR_OOM when it can never fit the budget, SB_ERR_TIMEOUT when
+ * the wait ran out) and its submit-to-done latency. Each ticket is waited once. */
+int sb_server_wait(sb_server* s, uint64_t ticket, int timeout_ms, double* latency_ms);
+int sb_server_stats_get(sb_server* s, sb_server_stats* out);
+/* Finishes every queued request, then stops the loop. */
+int sb_server_destroy(sb_server* s);
 
 #ifdef __cplusplus
 }

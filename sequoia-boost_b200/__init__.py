@@ -23,6 +23,7 @@ from .api import (  # noqa: F401
     GpuBackend,
     HistTreeBuilder,
     Monotone,
+    Server,
     TrainingParams,
     default_context,
     train,
@@ -31,5 +32,5 @@ from ._abi import SbError  # noqa: F401
 
 __all__ = [
     "BoostedModel", "Booster", "Context", "DMatrix", "GHistIndex", "GpuBackend",
-    "HistTreeBuilder", "Monotone", "SbError", "TrainingParams", "default_context", "train",
+    "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "train",
 ]

@@ -120,6 +120,15 @@ class SbBoosterStats(ctypes.Structure):
     ]
 
 
+class SbServerStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "submitted", "completed", "failed", "batches", "rows", "max_batch_requests", "memory_waits",
+        "mem_bytes", "mem_peak")]
+
+
+SB_REQ_MARGIN = 0
+SB_REQ_CONTRIBS = 1
+
 # name -> (restype, argtypes) of every symbol include/sb_gpu.h declares.
 P = ctypes.c_void_p
 SZ = ctypes.c_size_t
@@ -161,6 +170,7 @@ SIGNATURES = {
     "sb_booster_row_mask": (I32, [P, ctypes.c_uint64, U8P]),
     "sb_booster_model": (I32, [P, ctypes.POINTER(P)]),
     "sb_booster_destroy": (I32, [P]),
+    "sb_booster_set_graphs": (I32, [P, I32]),
     "sb_booster_set_timing": (I32, [P, I32]),
     "sb_booster_stats_get": (I32, [P, ctypes.POINTER(SbBoosterStats)]),
     "sb_booster_stats_reset": (I32, [P]),
@@ -174,6 +184,11 @@ SIGNATURES = {
     "sb_predict_margin": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, SZ, F32P]),
     "sb_predict": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P]),
     "sb_predict_contribs": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
+    "sb_server_create": (I32, [P, P, SZ, I32, ctypes.POINTER(P)]),
+    "sb_server_submit": (I32, [P, I32, F32P, SZ, SZ, ctypes.c_float, F32P, ctypes.POINTER(ctypes.c_uint64)]),
+    "sb_server_wait": (I32, [P, ctypes.c_uint64, I32, ctypes.POINTER(ctypes.c_double)]),
+    "sb_server_stats_get": (I32, [P, ctypes.POINTER(SbServerStats)]),
+    "sb_server_destroy": (I32, [P]),
 }
 
 

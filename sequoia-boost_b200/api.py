@@ -141,6 +141,7 @@ class Context:
         h = ctypes.c_void_p()
         A.check(A.lib().sb_ctx_create(device, ctypes.byref(h)))
         self.h = h
+        self.device = device
 
     def synchronize(self):
         A.check(A.lib().sb_ctx_synchronize(self.h))
@@ -560,6 +561,10 @@ class Booster:
     def set_timing(self, on=True):
         A.check(A.lib().sb_booster_set_timing(self.h, 1 if on else 0))
 
+    def set_graphs(self, on=True):
+        """Replay steady-state rounds as one CUDA graph each (default on)."""
+        A.check(A.lib().sb_booster_set_graphs(self.h, 1 if on else 0))
+
     def stats(self):
         s = A.SbBoosterStats()
         A.check(A.lib().sb_booster_stats_get(self.h, ctypes.byref(s)))
@@ -572,3 +577,57 @@ class Booster:
         if getattr(self, "h", None):
             A.lib().sb_booster_destroy(self.h)
             self.h = None
+
+
+class Server:
+    """The serving loop (sb_server): the model stays resident in HBM and margin
+    / TreeSHAP requests from any thread are batched continuously on the
+    device. `submit` returns a ticket; `wait` returns the request's output
+    (the same array as `predict_margin` / `predict_contribs` would give) and
+    its submit-to-done latency in ms."""
+
+    KINDS = {"margin": A.SB_REQ_MARGIN, "contribs": A.SB_REQ_CONTRIBS}
+
+    def __init__(self, model: BoostedModel, mem_bytes=0, n_slots=4, ctx: Context = None):
+        self.model = model  # must outlive the loop
+        self.ctx = ctx or model.ctx
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_server_create(self.ctx.h, model.h, mem_bytes, n_slots, ctypes.byref(h)))
+        self.h = h
+        self.k = model.n_outputs()
+        self.f = model.info()[2]
+        self._pending = {}
+
+    def submit(self, x, kind="margin", missing=float("nan"), out=None):
+        """Queues rows `x` [n][n_features] (kept referenced until `wait`)."""
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.f)
+        n = x.shape[0]
+        shape = (n, self.k) if kind == "margin" else (n, self.k, self.f + 1)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        t = ctypes.c_uint64()
+        A.check(A.lib().sb_server_submit(self.h, self.KINDS[kind], A.ptr(x, ctypes.c_float), n, self.f,
+                                         missing, A.ptr(out, ctypes.c_float), ctypes.byref(t)))
+        self._pending[t.value] = (x, out)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        lat = ctypes.c_double()
+        st = A.lib().sb_server_wait(self.h, ticket, timeout_ms, ctypes.byref(lat))
+        x, out = self._pending.pop(ticket)
+        A.check(st)
+        return out.reshape(-1), lat.value
+
+    def stats(self):
+        s = A.SbServerStats()
+        A.check(A.lib().sb_server_stats_get(self.h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            A.check(A.lib().sb_server_destroy(self.h))
+            self.h = None
+            self._pending.clear()
+
+    def __del__(self):
+        self.close()

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsb_gpu.so")
-SOURCES = ["sb_core.cu", "sb_bin.cu", "sb_hist.cu", "sb_grow.cu", "sb_predict.cu", "sb_static.cu"]
+SOURCES = ["sb_core.cu", "sb_bin.cu", "sb_hist.cu", "sb_grow.cu", "sb_predict.cu", "sb_static.cu", "sb_serve.cu"]
 HEADERS = ["sb_internal.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -46,7 +46,7 @@ def build(verbose=False, extra_flags=()):
             subprocess.run(cmd, check=True)
     if _newer(LIB, objs):
         cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
-               "-lcudart"]
+               "-lcudart", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

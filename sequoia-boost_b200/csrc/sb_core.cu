@@ -178,7 +178,7 @@ int sb_ctx_synchronize(sb_ctx* ctx) {
 }
 
 void* sb_ctx_stream(sb_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
-uint64_t sb_ctx_launch_count(const sb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+uint64_t sb_ctx_launch_count(const sb_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
 // ------------------------------------------------------------------ model
 int sb_model_create(sb_ctx* ctx, const sb_model_view* v, sb_model** out) {

@@ -1397,6 +1397,11 @@ struct sb_booster {
   sb::DBuf<float> d_margin, d_labels, d_weights;
   sb::DBuf<float> d_delta;   // [n][K] leaf values of the last tree, not yet in d_margin
   mutable bool delta_pending = false;  // margins are read through const handles
+  bool use_graphs = true;              // replay steady-state rounds as a CUDA graph
+  cudaGraphExec_t graph_exec = nullptr;
+  uint64_t graph_nodes = 0;            // kernels in the recorded round
+  sb::BState prev_key;                 // device state of the previous round
+  bool have_prev_key = false;
   sb::DBuf<float2> d_gpair;
   sb::DBuf<unsigned long long> d_gpk;
   sb::DBuf<unsigned int> d_maxabs;
@@ -1726,7 +1731,10 @@ size_t eval_smem(const sb_booster* b) {
   return b->S.cat_cap ? (EVAL_THREADS / 32) * sizeof(CatScratch) : 0;
 }
 
-int booster_round(sb_booster* b) {
+// The launches of one boosting round on the context stream (also recorded into
+// a CUDA graph by booster_round). Work sizes live in device memory, so the
+// sequence depends only on the booster's shape.
+int booster_round_body(sb_booster* b, int apply_delta) {
   sb_ctx* ctx = b->ctx;
   BState& S = b->S;
   cudaEvent_t r0 = nullptr, r1 = nullptr;
@@ -1740,10 +1748,9 @@ int booster_round(sb_booster* b) {
     SB_CUDA(cudaEventRecord(r0, ctx->stream));
   }
   const unsigned gblocks = (unsigned)std::min<size_t>((b->n + 255) / 256, (size_t)ctx->num_sms * 16);
-  S.apply_delta = b->delta_pending ? 1 : 0;
+  S.apply_delta = apply_delta;
   SB_LAUNCH(ctx, k_gradient, gblocks, 256, 0, S);
   S.apply_delta = 0;
-  b->delta_pending = S.update_margin != 0;
   SB_LAUNCH(ctx, k_round_prep, (unsigned)b->K, PREP_THREADS, 0, S);
   if (S.fixed) SB_LAUNCH(ctx, k_quantize, gblocks, 256, 0, S);
   HistLaunch L;
@@ -1800,6 +1807,50 @@ int booster_round(sb_booster* b) {
     b->ev.push_back(r1);
     b->ev_kind.push_back(1);
   }
+  return SB_OK;
+}
+
+// One boosting round. Once two consecutive rounds see the same device state
+// (buffers, shapes, whether the previous tree's leaf values are pending), the
+// round is recorded as a CUDA graph and replayed with one launch per round
+// until that state changes (for instance when the tree buffers grow).
+int booster_round(sb_booster* b) {
+  sb_ctx* ctx = b->ctx;
+  const int apply = b->delta_pending ? 1 : 0;
+  BState key;
+  std::memcpy(&key, &b->S, sizeof(BState));
+  key.apply_delta = apply;
+  const bool same = b->have_prev_key && std::memcmp(&key, &b->prev_key, sizeof(BState)) == 0;
+  std::memcpy(&b->prev_key, &key, sizeof(BState));
+  b->have_prev_key = true;
+  if (!b->use_graphs || b->timing || !same) {
+    if (b->graph_exec && !same) {
+      cudaGraphExecDestroy(b->graph_exec);
+      b->graph_exec = nullptr;
+    }
+    SB_TRY(booster_round_body(b, apply));
+  } else {
+    if (!b->graph_exec) {
+      const uint64_t l0 = ctx->launches;
+      SB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = booster_round_body(b, apply);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+      b->graph_nodes = ctx->launches - l0;
+      ctx->launches = l0;  // recorded, not launched
+      if (rc != SB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      SB_CUDA(e);
+      const cudaError_t ei = cudaGraphInstantiate(&b->graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      SB_CUDA(ei);
+    }
+    SB_CUDA(cudaGraphLaunch(b->graph_exec, ctx->stream));
+    ctx->launches += b->graph_nodes;
+  }
+  b->delta_pending = b->S.update_margin != 0;
   return SB_OK;
 }
 
@@ -2025,7 +2076,18 @@ int sb_booster_destroy(sb_booster* b) {
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
     for (auto e : b->ev) cudaEventDestroy(e);
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     delete b;
+  }
+  return SB_OK;
+}
+
+int sb_booster_set_graphs(sb_booster* b, int enable) {
+  SB_REQUIRE(b != nullptr, SB_ERR_INVALID_ARG, "booster is NULL");
+  b->use_graphs = enable != 0;
+  if (!b->use_graphs && b->graph_exec) {
+    cudaGraphExecDestroy(b->graph_exec);
+    b->graph_exec = nullptr;
   }
   return SB_OK;
 }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -47,13 +48,21 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
     SB_CUDA(cudaGetLastError());                                            \
   } while (0)
 
+// The same on another stream of the context's device.
+#define SB_LAUNCH_ON(ctx, st, kern, grid, block, smem, ...)                 \
+  do {                                                                      \
+    kern<<<(grid), (block), (smem), (st)>>>(__VA_ARGS__);                   \
+    (ctx)->launches++;                                                      \
+    SB_CUDA(cudaGetLastError());                                            \
+  } while (0)
+
 struct sb_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   size_t smem_optin = 0;     // max dynamic shared memory per block
   size_t smem_per_sm = 0;
-  uint64_t launches = 0;
+  std::atomic<uint64_t> launches{0};  // also counted by serving threads
 };
 
 namespace sb {

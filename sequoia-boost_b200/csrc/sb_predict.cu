@@ -428,6 +428,70 @@ int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, f
   return SB_OK;
 }
 
+// ---- batch launchers on an explicit stream with caller-owned buffers (used
+// by the serving loop; the model must be resident, see model_upload)
+
+size_t margin_chunk_rows(const sb_model* m) {
+  const size_t T = (size_t)std::max(m->dev.n_trees, 1);
+  return std::max<size_t>(1024, (size_t)(64ull << 20) / (T * 4));  // leaf buffer <= 64 MB
+}
+
+int margin_batch(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t F, float missing,
+                 float* d_buf, size_t buf_rows, float* d_out) {
+  sb_ctx* ctx = m->ctx;
+  const int Kc = m->num_class >= 2 ? m->num_class : 1;
+  const int T = m->dev.n_trees;
+  PredDev P;
+  P.nodes = m->dev.nodes.p;
+  P.cat_end = m->dev.cat_end.p;
+  P.tree_off = m->dev.tree_off.p;
+  P.cats = m->dev.cats.p;
+  P.weights = m->dev.weights.p;
+  P.n_trees = T;
+  for (size_t r0 = 0; r0 < n; r0 += buf_rows) {
+    const size_t nb = std::min(buf_rows, n - r0);
+    if (T > 0) {
+      const int tpb = 8;
+      dim3 grid((unsigned)((nb + 127) / 128), (unsigned)((T + tpb - 1) / tpb));
+      SB_LAUNCH_ON(ctx, st, k_leaf_values, grid, 128, 0, P, d_X + r0 * F, nb, (int)F, missing, T, tpb, d_buf);
+    }
+    const size_t tot = nb * Kc;
+    SB_LAUNCH_ON(ctx, st, k_margin_sum, (unsigned)((tot + 255) / 256), 256, 0, P, d_buf, nb, Kc, T,
+                 m->base_score, (const float*)nullptr, 0, d_out + r0 * Kc);
+  }
+  return SB_OK;
+}
+
+int contribs_bias(sb_model* m, std::vector<double>* bias) {
+  SB_TRY(model_upload(m));
+  const int K = m->num_class >= 2 ? m->num_class : 1;
+  bias->assign(K, (double)m->base_score);
+  for (size_t t = 0; t < m->trees.size(); ++t) (*bias)[t % K] += node_mean_value(m->trees[t], 0);
+  return SB_OK;
+}
+
+int contribs_batch(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t F, float missing,
+                   double* d_acc, const double* d_bias, float* d_out) {
+  sb_ctx* ctx = m->ctx;
+  SB_REQUIRE(m->dev.max_depth <= SHAP_MAXD, SB_ERR_UNSUPPORTED,
+             "TreeSHAP on the device supports trees up to depth %d (got %d)", SHAP_MAXD, m->dev.max_depth);
+  const int K = m->num_class >= 2 ? m->num_class : 1;
+  const int T = m->dev.n_trees;
+  const size_t tot = n * K * (F + 1);
+  SB_CUDA(cudaMemsetAsync(d_acc, 0, tot * sizeof(double), st));
+  ShapDev P;
+  P.nodes = m->dev.full.p;
+  P.tree_off = m->dev.tree_off.p;
+  P.n_trees = T;
+  if (T > 0 && n > 0) {
+    const int tpb = 4;
+    dim3 grid((unsigned)((n + 63) / 64), (unsigned)((T + tpb - 1) / tpb));
+    SB_LAUNCH_ON(ctx, st, k_shap, grid, 64, 0, P, d_X, n, (int)F, K, missing, tpb, d_acc);
+  }
+  if (tot) SB_LAUNCH_ON(ctx, st, k_shap_finish, (unsigned)((tot + 255) / 256), 256, 0, d_acc, d_bias, n, K, (int)F, d_out);
+  return SB_OK;
+}
+
 }  // namespace sb
 
 extern "C" {

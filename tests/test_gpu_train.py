@@ -133,3 +133,27 @@ def test_zero_rounds_and_base_score(sb, ctx):
     m = sb.train(p, sb.DMatrix(x, labels=y), 0, ctx=ctx)
     assert m.num_trees() == 0
     assert np.all(m.predict(sb.DMatrix(x)) == np.float32(0.5))
+
+
+def test_graph_replayed_rounds_match_eager_rounds(sb, ctx):
+    """Rounds replayed from a recorded CUDA graph give the same trees and
+    margins as rounds launched kernel by kernel, across a tree-buffer growth
+    (the graph is re-recorded) and a host read of the margins mid-way."""
+    x, _ = mixed_data(30000, 16, seed=8)
+    y = (np.nan_to_num(x[:, 0]) + 0.5 * np.nan_to_num(x[:, 1]) > 0).astype(np.float32)
+    p = sb.TrainingParams(objective="binary:logistic", max_depth=6, eta=0.3, subsample=0.8,
+                          colsample_bytree=0.8, hist_precision="fixed", seed=5)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    out = []
+    for graphs in (True, False):
+        b = sb.Booster(gh, p, y)
+        b.set_graphs(graphs)
+        for r in range(20):
+            b.update(1)
+            if r == 9:
+                mid = b.margins().copy()
+        out.append((b.model().export(), mid, b.margins()))
+    (ma, mida, fa), (mb, midb, fb) = out
+    assert_trees_equal(ma, mb)
+    assert np.array_equal(mida, midb)
+    assert np.array_equal(fa, fb)
