@@ -50,9 +50,27 @@ struct Fill {
 
 struct FeatRec;
 
+// An entry of a lossguide tree's priority queue (NodeEntry ordered by
+// loss_chg.total_cmp, hist.rs:79-95).
+struct HeapEnt {
+  long long key;  // total_cmp_key(loss_chg)
+  int nid;
+  int depth;
+};
+
 struct BState {
   // shapes
   int K, F, FW, HB, total_bins, max_depth, maxn, maxw, cat_cap;
+  // lossguide growth (grow_lossguide, hist.rs:238-268)
+  int lossguide;
+  int max_leaves;           // leaf budget (2^max_depth when max_leaves is 0)
+  int depth_limit;          // max_depth, or INT_MAX for 0
+  char* nhist;              // [K][maxn][HB] x 16 B: every node's histogram
+  HeapEnt* heap;            // [K][maxn]
+  int* heap_size;           // [K]
+  int* n_leaves;            // [K]
+  int* ndepth;              // [K][maxn]
+  int* prev_count;          // [K] frontier nodes expanded by the last k_assign
   size_t n, Fp;
   // binned data
   const uint16_t* bins;      // tile-relative codes, row-major
@@ -151,6 +169,20 @@ __device__ __forceinline__ size_t NI(const BState& S, int k, int nid) { return (
 __device__ __forceinline__ char* level_hist(const BState& S, int d, int k, int slot) {
   char* base = (d & 1) ? S.hist1 : S.hist0;
   return base + ((size_t)k * S.maxw + slot) * (size_t)S.HB * 16;
+}
+
+__device__ __forceinline__ char* node_hist(const BState& S, int k, int nid) {
+  return S.nhist + NI(S, k, nid) * (size_t)S.HB * 16;
+}
+
+// Histogram of frontier slot `slot` of tree k at level d (lossguide: of the node).
+__device__ __forceinline__ char* frontier_hist(const BState& S, int d, int k, int slot) {
+  return S.lossguide ? node_hist(S, k, S.lvl_begin[k] + slot) : level_hist(S, d, k, slot);
+}
+
+// Histogram of the parent of node index ni (a node of frontier level d).
+__device__ __forceinline__ const char* parent_hist(const BState& S, int d, int k, size_t ni) {
+  return S.lossguide ? node_hist(S, k, S.parent[ni]) : level_hist(S, d - 1, k, S.parent[ni] - S.prev_begin[k]);
 }
 
 template <typename T>
@@ -386,7 +418,9 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
     S.lvl_begin[k] = 0;
     S.lvl_count[k] = 1;
     S.prev_begin[k] = 0;
+    S.prev_count[k] = 0;
     S.cat_count[k] = 0;
+    if (S.lossguide) S.ndepth[NI(S, k, 0)] = 0;
     const size_t r0 = NI(S, k, 0);
     S.seg[r0] = make_uint2(0u, (unsigned)S.n);
     S.nsamp[r0] = *S.kept;
@@ -401,7 +435,7 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
     it.end = (uint32_t)S.n;
     it.k = (uint32_t)k;
     it.root = 1;
-    it.out = level_hist(S, 0, k, 0);
+    it.out = S.lossguide ? node_hist(S, k, 0) : level_hist(S, 0, k, 0);
     it.total = &S.root_total[k];
     S.items[k] = it;
     S.prefix[k] = (uint64_t)k * S.n;
@@ -793,11 +827,10 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) {
   const int f = (int)S.upool[(size_t)k * S.F + pi];
   const int nid = S.lvl_begin[k] + slot;
   const size_t ni = NI(S, k, nid);
-  char* H = level_hist(S, d, k, slot);
+  char* H = frontier_hist(S, d, k, slot);
   if (d > 0 && !S.built[ni]) {
-    const int pslot = S.parent[ni] - S.prev_begin[k];
-    const char* P = level_hist(S, d - 1, k, pslot);
-    const char* B = level_hist(S, d, k, slot ^ 1);
+    const char* P = parent_hist(S, d, k, ni);
+    const char* B = frontier_hist(S, d, k, slot ^ 1);
     const int fs = (int)S.foff[f], nb = (int)S.foff[f + 1] - fs;
     for (int i = lane; i <= nb; i += 32) {
       const int e = i < nb ? fs + i : S.total_bins + f;  // bins, then the missing bin
@@ -851,7 +884,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) 
   q = warp_max(q);
   const EvalNode E = eval_node(S, k, ni, d);
   CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
-  scan_feature<SCAN_RECORDS>(S, level_hist(S, d, k, slot), k, f, E, q, cs, s_gains[warp], nullptr, rec);
+  scan_feature<SCAN_RECORDS>(S, frontier_hist(S, d, k, slot), k, f, E, q, cs, s_gains[warp], nullptr, rec);
 }
 
 // Phase 2b, one warp per frontier node: the winner of consider's sequential
@@ -866,7 +899,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
   if (slot >= S.lvl_count[k]) return;
   const int nid = S.lvl_begin[k] + slot;
   const size_t ni = NI(S, k, nid);
-  const char* H = level_hist(S, d, k, slot);
+  const char* H = frontier_hist(S, d, k, slot);
   const EvalNode E = eval_node(S, k, ni, d);
   NodeSplit* best = &s_best[warp];
   const double* M = S.mbuf + ((size_t)k * S.maxw + slot) * S.F;
@@ -978,7 +1011,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
   const int tid = threadIdx.x;
   if (tid == 0) s_tile_carry = 0;
   __syncthreads();
-  const bool last = (d + 1 == S.max_depth);
+  const bool last = !S.lossguide && (d + 1 == S.max_depth);
   for (int k = 0; k < S.K; ++k) {
     const int begin = S.lvl_begin[k], cnt = S.lvl_count[k], nn0 = S.num_nodes[k];
     const size_t t = (size_t)round * S.K + k;
@@ -1109,6 +1142,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
     __syncthreads();
     if (tid == 0) {
       S.prev_begin[k] = begin;
+      S.prev_count[k] = cnt;
       S.lvl_begin[k] = nn0;
       S.lvl_count[k] = 2 * carry_v;
       S.num_nodes[k] = nn0 + 2 * carry_v;
@@ -1133,10 +1167,11 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
   __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
   __shared__ uint2 s_ws[PART_WARPS];
   __shared__ unsigned int s_base[2];
-  const bool last = (d + 1 == S.max_depth);
+  const bool last = !S.lossguide && (d + 1 == S.max_depth);
   const int ntiles = *S.ptile_count;
-  const uint32_t* rows_cur_all = (d & 1) ? S.rows1 : S.rows0;
-  uint32_t* rows_nxt_all = (d & 1) ? S.rows0 : S.rows1;
+  // lossguide: from the tree's list into the scratch list (k_lg_copy moves it back)
+  const uint32_t* rows_cur_all = (!S.lossguide && (d & 1)) ? S.rows1 : S.rows0;
+  uint32_t* rows_nxt_all = (!S.lossguide && (d & 1)) ? S.rows0 : S.rows1;
   const int K = S.K;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
@@ -1268,9 +1303,9 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
   const int dn = d + 1;
   for (int k = 0; k < S.K; ++k) {
     const int pbegin = S.prev_begin[k];
-    const int pcount = S.lvl_begin[k] - pbegin;  // frontier of level d
+    const int pcount = S.prev_count[k];  // frontier of level d
     const int cbegin = S.lvl_begin[k];
-    uint32_t* rows_nxt = ((dn & 1) ? S.rows1 : S.rows0) + (size_t)k * S.n;
+    uint32_t* rows_nxt = ((!S.lossguide && (dn & 1)) ? S.rows1 : S.rows0) + (size_t)k * S.n;
     const sb_node* out = S.out_nodes + ((size_t)round * S.K + k) * S.maxn;
     for (int c0 = 0; c0 < pcount; c0 += blockDim.x) {
       const int slot = c0 + tid;
@@ -1310,7 +1345,7 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
         it.end = bseg.y;
         it.k = (uint32_t)k;
         it.root = 0;
-        it.out = level_hist(S, dn, k, bchild - cbegin);
+        it.out = S.lossguide ? node_hist(S, k, bchild) : level_hist(S, dn, k, bchild - cbegin);
         it.total = nullptr;
         S.items[idx] = it;
         S.prefix[idx] = pos;
@@ -1326,6 +1361,144 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
   if (tid == 0) {
     *S.item_count = s_items;
     S.prefix[s_items] = s_pos;
+  }
+}
+
+// ------------------------------------------------------- lossguide growth
+// grow_lossguide (hist.rs:238-268): per class tree, a max-heap of evaluated
+// nodes keyed by loss_chg; each step pops the next node to expand, and the
+// step's kernels (assign, partition, histogram of the smaller child,
+// evaluation of both children) run for all K trees at once.
+
+// One block per class tree. Pushes the children evaluated by the last step
+// (or the root, `init`), then pops until a node that may be split: the steps
+// of Rust's BinaryHeap (sift_up on push; swap with the last entry,
+// sift_down_to_bottom and sift_up on pop), run by one thread on a
+// shared-memory copy of the queue, so equal keys leave in the same order.
+__global__ void __launch_bounds__(256) k_lg_heap(BState S, int init) {
+  extern __shared__ HeapEnt sh_heap[];  // [maxn]
+  __shared__ int s_size;
+  const int k = blockIdx.x, tid = threadIdx.x;
+  HeapEnt* gh = S.heap + (size_t)k * S.maxn;
+  if (tid == 0) s_size = init ? 0 : S.heap_size[k];
+  __syncthreads();
+  const int size0 = s_size;
+  for (int i = tid; i < size0; i += blockDim.x) sh_heap[i] = gh[i];
+  __syncthreads();
+  if (tid == 0) {
+    HeapEnt* h = sh_heap;
+    int size = size0;
+    auto sift_up = [&](int start, int pos) {
+      const HeapEnt hole = h[pos];
+      while (pos > start) {
+        const int par = (pos - 1) / 2;
+        if (hole.key <= h[par].key) break;
+        h[pos] = h[par];
+        pos = par;
+      }
+      h[pos] = hole;
+    };
+    auto push = [&](HeapEnt e) {
+      h[size] = e;
+      size++;
+      sift_up(0, size - 1);
+    };
+    auto pop = [&]() {
+      HeapEnt item = h[size - 1];
+      size--;
+      if (size > 0) {
+        const HeapEnt top = h[0];
+        h[0] = item;
+        item = top;
+        // sift_down_to_bottom(0)
+        const int end = size;
+        int pos = 0;
+        const HeapEnt hole = h[0];
+        int child = 1;
+        while (end >= 2 && child <= end - 2) {
+          child += (h[child].key <= h[child + 1].key) ? 1 : 0;
+          h[pos] = h[child];
+          pos = child;
+          child = 2 * pos + 1;
+        }
+        if (child == end - 1) {
+          h[pos] = h[child];
+          pos = child;
+        }
+        h[pos] = hole;
+        sift_up(0, pos);
+      }
+      return item;
+    };
+    sb_node* out = S.out_nodes + ((size_t)(*S.round) * S.K + k) * S.maxn;
+    if (init) {
+      const size_t r = NI(S, k, 0);
+      out[0] = make_leaf(0.0f, (float)S.stats[r].y);  // RegTree::with_root
+      push(HeapEnt{total_cmp_key(S.split[r].loss_chg), 0, 0});
+      S.n_leaves[k] = 1;
+    } else if (S.prev_count[k] > 0) {  // heap.push(l); heap.push(r)
+      for (int c = 0; c < S.lvl_count[k]; ++c) {
+        const int nid = S.lvl_begin[k] + c;
+        const size_t ni = NI(S, k, nid);
+        const int dep = S.ndepth[NI(S, k, S.parent[ni])] + 1;
+        S.ndepth[ni] = dep;
+        push(HeapEnt{total_cmp_key(S.split[ni].loss_chg), nid, dep});
+      }
+    }
+    int expand = -1, nl = S.n_leaves[k];
+    while (size > 0) {
+      const HeapEnt e = pop();
+      if (nl >= S.max_leaves) {
+        size = 0;
+        break;
+      }
+      if (e.depth >= S.depth_limit || !S.split[NI(S, k, e.nid)].valid) continue;  // permanent leaf
+      expand = e.nid;
+      nl++;  // one leaf becomes two
+      break;
+    }
+    S.n_leaves[k] = nl;
+    S.lvl_begin[k] = expand >= 0 ? expand : S.num_nodes[k];
+    S.lvl_count[k] = expand >= 0 ? 1 : 0;
+    s_size = size;
+  }
+  __syncthreads();
+  const int size1 = s_size;
+  for (int i = tid; i < size1; i += blockDim.x) gh[i] = sh_heap[i];
+  if (tid == 0) S.heap_size[k] = size1;
+}
+
+// The expanded node's partitioned rows back into the tree's row list.
+__global__ void k_lg_copy(BState S) {
+  const int ntiles = *S.ptile_count;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int4 tile = S.ptiles[t];
+    const size_t base = (size_t)tile.x * S.n;
+    for (int p = tile.z + threadIdx.x; p < tile.w; p += blockDim.x) S.rows0[base + p] = S.rows1[base + p];
+  }
+}
+
+// Leaf values of every leaf (hist.rs:193-200 then scale_leaves) and the
+// leaf value of each of its rows (the margin update, train.rs:326-328).
+__global__ void k_lg_finalize(BState S) {
+  const int k = blockIdx.y, nid = blockIdx.x;
+  if (nid >= S.num_nodes[k]) return;
+  const size_t ni = NI(S, k, nid);
+  sb_node* out = S.out_nodes + ((size_t)(*S.round) * S.K + k) * S.maxn;
+  if (out[nid].left != -1) return;
+  const double2 st = S.stats[ni], bd = S.bounds[ni];
+  const float lv = __fmul_rn((float)calc_weight_bounded(st.x, st.y, S.reg, bd.x, bd.y), S.eta);
+  if (threadIdx.x == 0) {
+    out[nid].leaf_value = lv;
+    S.leafval[ni] = lv;
+  }
+  const uint2 sg = S.seg[ni];
+  const uint32_t* rows = S.rows0 + (nid == 0 ? 0 : (size_t)k * S.n);  // an unsplit root keeps the shared list
+  for (uint32_t p = sg.x + threadIdx.x; p < sg.y; p += blockDim.x) {
+    const uint32_t rv = rows[p];
+    const uint32_t id = rv & ~UNSAMPLED;
+    if (S.update_margin) S.delta[(size_t)id * S.K + k] = lv;
+    if (S.row_leaf) S.row_leaf[id] = (rv & UNSAMPLED) ? -1 : nid;
   }
 }
 
@@ -1409,6 +1582,12 @@ struct sb_booster {
   sb::DBuf<double> d_inv_scale;
   sb::DBuf<unsigned long long> d_qerr;
   sb::DBuf<char> d_hist0, d_hist1;
+  bool lossguide = false;
+  int leaves = 0, steps = 0;              // lossguide: leaf budget, expansions per tree
+  sb::DBuf<char> d_nhist;                 // lossguide: [K][maxn][HB] node histograms
+  sb::DBuf<sb::HeapEnt> d_heap;           // lossguide: [K][maxn] queues
+  sb::DBuf<int> d_heap_size;              // lossguide: [K] sizes, then [K] leaf counts
+  sb::DBuf<int> d_ndepth;                 // lossguide: [K][maxn] node depths
   sb::DBuf<longlong2> d_root_total;
   sb::DBuf<sb::HistItem> d_items;
   sb::DBuf<uint64_t> d_prefix;
@@ -1533,12 +1712,19 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   b->n = g->n;
   const int F = (int)g->F;
   const int FW = (F + 31) / 32;
-  SB_REQUIRE(p->grow_policy == SB_GROW_DEPTHWISE, SB_ERR_UNSUPPORTED,
-             "grow_policy=lossguide is not available on the GPU path yet");
   SB_REQUIRE(K >= 1 && K <= 16, SB_ERR_UNSUPPORTED, "at most 16 outputs per round on the GPU");
+  b->lossguide = p->grow_policy == SB_GROW_LOSSGUIDE;
   b->D = p->max_depth;
-  b->maxn = (1 << (b->D + 1)) - 1;
-  b->maxw = 1 << (b->D - 1);
+  if (b->lossguide) {  // one node expanded per tree and step
+    b->leaves = p->max_leaves > 0 ? p->max_leaves : (1 << p->max_depth);
+    b->steps = b->leaves - 1;
+    if (p->max_depth > 0 && p->max_depth < 31) b->steps = std::min(b->steps, (1 << p->max_depth) - 1);
+    b->maxn = 2 * b->leaves - 1;
+    b->maxw = 2;
+  } else {
+    b->maxn = (1 << (b->D + 1)) - 1;
+    b->maxw = 1 << (b->D - 1);
+  }
   if (p->n_monotone > 0 && p->monotone) b->mono.assign(p->monotone, p->monotone + p->n_monotone);
   bool constrained = false;
   for (int8_t m : b->mono) constrained |= m != 0;
@@ -1585,7 +1771,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   SB_CUDA(cudaMemsetAsync(b->d_split.p, 0, b->d_split.bytes(), st));
   SB_TRY(b->d_leafval.alloc(ctx, KN));
   SB_TRY(b->d_fill.alloc(ctx, KN));
-  SB_TRY(b->d_lvl.alloc(ctx, 5 * K));
+  SB_TRY(b->d_lvl.alloc(ctx, 6 * K));
   SB_TRY(b->d_rows0.alloc(ctx, (size_t)K * b->n));
   SB_TRY(b->d_rows1.alloc(ctx, (size_t)K * b->n));
   SB_TRY(b->d_kept.alloc(ctx, 1));
@@ -1602,9 +1788,16 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   SB_TRY(b->d_inv_scale.alloc(ctx, 2 * K));
   SB_TRY(b->d_qerr.alloc(ctx, 1));
   SB_CUDA(cudaMemsetAsync(b->d_qerr.p, 0, 8, st));
-  const size_t hist_bytes = (size_t)K * b->maxw * HB * 16;
-  SB_TRY(b->d_hist0.alloc(ctx, hist_bytes));
-  SB_TRY(b->d_hist1.alloc(ctx, hist_bytes));
+  if (b->lossguide) {  // every node keeps its histogram until its children are evaluated
+    SB_TRY(b->d_nhist.alloc(ctx, KN * HB * 16));
+    SB_TRY(b->d_heap.alloc(ctx, KN));
+    SB_TRY(b->d_heap_size.alloc(ctx, 2 * K));
+    SB_TRY(b->d_ndepth.alloc(ctx, KN));
+  } else {
+    const size_t hist_bytes = (size_t)K * b->maxw * HB * 16;
+    SB_TRY(b->d_hist0.alloc(ctx, hist_bytes));
+    SB_TRY(b->d_hist1.alloc(ctx, hist_bytes));
+  }
   SB_TRY(b->d_root_total.alloc(ctx, K));
   SB_TRY(b->d_items.alloc(ctx, (size_t)K * b->maxw + K));
   SB_TRY(b->d_prefix.alloc(ctx, (size_t)K * b->maxw + K + 1));
@@ -1640,6 +1833,14 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.max_depth = b->D;
   S.maxn = b->maxn;
   S.maxw = b->maxw;
+  S.lossguide = b->lossguide ? 1 : 0;
+  S.max_leaves = b->lossguide ? b->leaves : 0;
+  S.depth_limit = p->max_depth > 0 ? p->max_depth : 0x7FFFFFFF;
+  S.nhist = b->d_nhist.p;
+  S.heap = b->d_heap.p;
+  S.heap_size = b->d_heap_size.p;
+  S.n_leaves = b->d_heap_size.p ? b->d_heap_size.p + K : nullptr;
+  S.ndepth = b->d_ndepth.p;
   S.cat_cap = g->has_categorical ? (b->maxn / 2 + 1) * g->max_feature_bins : 0;
   S.n = b->n;
   S.Fp = g->Fp;
@@ -1690,6 +1891,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.prev_begin = b->d_lvl.p + 2 * K;
   S.num_nodes = b->d_lvl.p + 3 * K;
   S.cat_count = b->d_lvl.p + 4 * K;
+  S.prev_count = b->d_lvl.p + 5 * K;
   S.rows0 = b->d_rows0.p;
   S.rows1 = b->d_rows1.p;
   S.kept = b->d_kept.p;
@@ -1785,7 +1987,33 @@ int booster_round_body(sb_booster* b, int apply_delta) {
     return SB_OK;
   };
   SB_TRY(hist(b->K));
-  for (int d = 0; d < b->D; ++d) {
+  if (b->lossguide) {
+    const unsigned fy = (unsigned)((b->g->F + SCAN_WARPS - 1) / SCAN_WARPS);
+    const size_t heap_smem = (size_t)b->maxn * sizeof(HeapEnt);
+    auto eval = [&](int d, unsigned width) -> int {
+      dim3 sg(width, fy, (unsigned)b->K);
+      SB_LAUNCH(ctx, k_eval_scan, sg, EVAL_THREADS, esm, S, d);
+      SB_LAUNCH(ctx, k_eval_records, sg, EVAL_THREADS, esm, S, d);
+      dim3 pg(1, (unsigned)b->K);
+      SB_LAUNCH(ctx, k_eval_pick, pg, EVAL_THREADS, esm, S, d);
+      return SB_OK;
+    };
+    SB_TRY(eval(0, 1));  // the root
+    SB_LAUNCH(ctx, k_lg_heap, (unsigned)b->K, 256, heap_smem, S, 1);
+    const unsigned pblocks = (unsigned)ctx->num_sms * 8;
+    for (int step = 0; step < b->steps; ++step) {
+      const int d = step == 0 ? 0 : 1;  // only the first expansion reads the shared root list
+      SB_LAUNCH(ctx, k_assign, 1, 1024, 0, S, d, 1);
+      SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
+      SB_LAUNCH(ctx, k_lg_copy, pblocks, 256, 0, S);
+      SB_LAUNCH(ctx, k_plan, 1, 1024, 0, S, d);
+      SB_TRY(hist(b->K));
+      SB_TRY(eval(1, 2));
+      SB_LAUNCH(ctx, k_lg_heap, (unsigned)b->K, 256, heap_smem, S, 0);
+    }
+    SB_LAUNCH(ctx, k_lg_finalize, dim3((unsigned)b->maxn, (unsigned)b->K), 256, 0, S);
+  }
+  for (int d = 0; d < b->D && !b->lossguide; ++d) {
     const unsigned width = (unsigned)std::min(1 << d, b->maxw);
     dim3 sg(width, (unsigned)((b->g->F + SCAN_WARPS - 1) / SCAN_WARPS), (unsigned)b->K);
     SB_LAUNCH(ctx, k_eval_scan, sg, EVAL_THREADS, esm, S, d);
@@ -1887,6 +2115,12 @@ int booster_set_eval_smem(sb_booster* b) {
   SB_CUDA(cudaFuncSetAttribute(k_eval_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
   SB_CUDA(cudaFuncSetAttribute(k_eval_pick, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
   SB_CUDA(cudaFuncSetAttribute(k_eval_records, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
+  if (b->lossguide) {
+    const size_t heap_smem = (size_t)b->maxn * sizeof(HeapEnt);
+    SB_REQUIRE(heap_smem <= b->ctx->smem_optin, SB_ERR_UNSUPPORTED, "lossguide queue of %d nodes exceeds shared memory",
+               b->maxn);
+    SB_CUDA(cudaFuncSetAttribute(k_lg_heap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heap_smem));
+  }
   return SB_OK;
 }
 
