@@ -31,6 +31,12 @@ import time
 
 import numpy as np
 
+# The serving loop keeps several streams in flight; with the default 8
+# hardware work queues, streams alias onto shared queues and a margin kernel
+# can wait behind a TreeSHAP kernel of another stream. Must be set before the
+# process's first CUDA call.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "train Mrow-rounds/s at matched RMSE; serving predict p50/p99 ms vs plain GPU"
@@ -50,6 +56,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-train-rows", type=int, default=1_000_000)
     return ap.parse_args()
 
 
@@ -150,6 +160,115 @@ def cpu_leg(x, y, args, sb, threads, rounds, rows):
         orc.train(xs, ys, p, 1, threads=threads, data=d)
         times.append(time.perf_counter() - t0)
     return xs.shape[0], times, t_bin
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
+
+
+def _latency_summary(lat, rows, kinds, wall):
+    lat = np.asarray(lat)
+    m = kinds == 0
+    small = m & (rows <= 4096)
+    return {"p50_ms_margin": _pct(lat[m], 50), "p99_ms_margin": _pct(lat[m], 99),
+            "p99_ms_margin_le4096_rows": _pct(lat[small], 99),
+            "p50_ms_contribs": _pct(lat[~m], 50), "p99_ms_contribs": _pct(lat[~m], 99),
+            "rows_per_s": float(rows.sum() / wall)}
+
+
+def serving_leg(sb, ctx, args, torch):
+    """The serving workload: a 1000-tree depth-8 ensemble trained on the
+    binary_mixed data (100 features), a Poisson request stream, rows per
+    request log-uniform in [1, 65536] (N(0,1) with 10% NaN), 90% margin and
+    10% TreeSHAP. Continuous batching (sb_server) against the same stream
+    served one request at a time by sb_predict_margin / sb_predict_contribs
+    ("plain GPU"). Latency = scheduled arrival to result on the host."""
+    import threading
+    from sequoia_boost_b200 import datagen
+    n = args.serve_train_rows
+    x, y = datagen.binary_mixed(n=n, seed=args.seed + 100)
+    xd = torch.from_numpy(x).to(f"cuda:{ctx.device}")
+    gh = sb.GHistIndex.from_device(xd.data_ptr(), n, x.shape[1], max_bin=256, ctx=ctx)
+    del xd
+    b = sb.Booster(gh, params_for(sb, "fixed"), y, ctx=ctx)
+    b.update(1000)
+    model = b.model()
+    del b, gh, x, y
+    F = 100
+    rng = np.random.default_rng(args.seed + 200)
+    pool = rng.standard_normal((65536, F)).astype(np.float32)
+    pool[rng.random(pool.shape) < 0.1] = np.nan
+    pool = torch.from_numpy(pool).pin_memory().numpy()
+    N = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, N))
+    rows = np.clip(np.exp(rng.uniform(0.0, np.log(65536.0), N)).astype(np.int64), 1, 65536)
+    kinds = (rng.random(N) < 0.1).astype(np.int64)  # 1 = TreeSHAP
+    offs = np.array([rng.integers(0, 65536 - r + 1) for r in rows])
+    outs = [torch.empty(int(r) * (1 if k == 0 else F + 1), dtype=torch.float32).pin_memory().numpy()
+            for r, k in zip(rows, kinds)]
+
+    def run_batched():
+        srv = sb.Server(model, mem_bytes=0, n_slots=8, ctx=ctx)
+        for i in range(8):  # warm-up
+            srv.wait(srv.submit(pool[:512], kind="contribs" if i % 4 == 3 else "margin"))
+        tickets = [None] * N
+        sub = np.zeros(N)
+        t0 = time.perf_counter() + 0.01
+
+        def submitter():
+            for i in range(N):
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                sub[i] = time.perf_counter()
+                lo = int(offs[i])
+                tickets[i] = srv.submit(pool[lo:lo + rows[i]], kind="contribs" if kinds[i] else "margin",
+                                        out=outs[i])
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat = np.zeros(N)
+        for i in range(N):
+            while tickets[i] is None:
+                time.sleep(0.0001)
+            _, l_ms = srv.wait(tickets[i])
+            lat[i] = l_ms + (sub[i] - (t0 + arrivals[i])) * 1e3
+        th.join()
+        wall = max(time.perf_counter() - t0, 1e-9)
+        st = srv.stats()
+        srv.close()
+        out = _latency_summary(lat, rows, kinds, wall)
+        out.update({"batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
+                    "memory_waits": st["memory_waits"], "mem_budget_bytes": st["mem_bytes"],
+                    "mem_peak_bytes": st["mem_peak"]})
+        return out
+
+    def run_plain():
+        for _ in range(4):
+            model.predict_margin(sb.DMatrix(pool[:512]))
+        model.predict_contribs(sb.DMatrix(pool[:512]))
+        lat = np.zeros(N)
+        t0 = time.perf_counter() + 0.01
+        for i in range(N):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            lo = int(offs[i])
+            dm = sb.DMatrix(pool[lo:lo + rows[i]])
+            if kinds[i]:
+                model.predict_contribs(dm)
+            else:
+                model.predict_margin(dm)
+            lat[i] = (time.perf_counter() - (t0 + arrivals[i])) * 1e3
+        wall = max(time.perf_counter() - t0, 1e-9)
+        return _latency_summary(lat, rows, kinds, wall)
+
+    batched = run_batched()
+    plain = run_plain()
+    return {"workload": f"1000-tree depth-8 binary:logistic ensemble (trained on {n} binary_mixed rows), "
+                        f"{N} requests, Poisson {args.serve_rate:g} req/s, rows log-uniform [1, 65536], "
+                        "10% NaN, 90% margin / 10% TreeSHAP",
+            "batched": batched, "plain_gpu": plain,
+            "requests_margin": int((kinds == 0).sum()), "requests_contribs": int(kinds.sum())}
 
 
 def run_reference(args):
@@ -290,13 +409,17 @@ def main():
                "kind": "port",
                "sample": f"first {rows} rows, {len(times)} rounds, binning excluded "
                          f"(binning {t_bin:.1f} s single-threaded)"}
+    serving = None
+    if not args.no_serve and rank == 0:
+        serving = serving_leg(sb, ctx, args, torch)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "i64" if args.precision == "fixed" else "f32", "data": "synthetic",
                 "config": config_of(args, n), "clocks": clk, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "quality": quality}
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "quality": quality,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -322,9 +322,13 @@ int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_col
  * from any number of threads, with continuous batching: a dispatcher thread
  * joins runs of queued requests of one kind into device batches, admits a
  * batch when its buffers fit in the free part of the loop's memory budget,
- * and keeps up to n_slots batches in flight on their own streams (margins at
- * high stream priority, TreeSHAP at low). Host buffers may be pageable;
- * page-locked X and out make the copies asynchronous. */
+ * and keeps up to n_slots margin batches (high stream priority) and
+ * max(1, n_slots / 2) TreeSHAP batches (low priority) in flight, each on its
+ * own stream. Host buffers may be pageable; page-locked X and out make the
+ * copies asynchronous. Set CUDA_DEVICE_MAX_CONNECTIONS to at least
+ * 1.5 * n_slots + 2 (e.g. 32) in the environment before the process's first
+ * CUDA call: with the default 8 hardware work queues, streams share queues and
+ * a margin batch can wait behind a TreeSHAP kernel of another stream. */
 typedef struct sb_server sb_server;
 enum { SB_REQ_MARGIN = 0, SB_REQ_CONTRIBS = 1 };
 typedef struct sb_server_stats {
@@ -335,7 +339,8 @@ typedef struct sb_server_stats {
   uint64_t mem_bytes, mem_peak;  /* budget and the most of it in use */
 } sb_server_stats;
 /* mem_bytes: device memory for request buffers (0 = half of what is free
- * now); n_slots: batches in flight (1..64). The model must outlive the loop. */
+ * now); n_slots: margin batches in flight (1..64). The model must outlive
+ * the loop. */
 int sb_server_create(sb_ctx* ctx, sb_model* m, size_t mem_bytes, int n_slots, sb_server** out);
 /* Queues a request; X [n_rows][n_cols] and out stay owned by the caller and
  * must stay valid until sb_server_wait returns for the ticket. */

@@ -46,7 +46,7 @@ def build(verbose=False, extra_flags=()):
             subprocess.run(cmd, check=True)
     if _newer(LIB, objs):
         cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
-               "-lcudart", "-lpthread"]
+               "-lcudart", "-lpthread", "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -175,16 +175,34 @@ struct HostTree {
   std::vector<uint32_t> cats;
 };
 
+// One element of a root-to-leaf path for TreeSHAP: every split on the path
+// that tests feature f, merged. A row follows the element when its value lies
+// in [lo, hi), or when it is missing and every such split sends missing
+// values the path's way. z = the product of the splits' cover fractions.
+struct PathEl {
+  int f;        // -1 for the path's first (bias) element
+  int miss_ok;
+  float lo, hi;
+  double z, inv_z;
+};
+
 struct DevEnsemble {
   DBuf<int4> nodes;          // packed predict nodes
   DBuf<int> cat_end;         // per node: end of its category list
   DBuf<int64_t> tree_off;    // node offset per tree
   DBuf<uint32_t> cats;
   DBuf<float> weights;
-  DBuf<sb_node> full;        // full nodes (SHAP)
   DBuf<double> tree_mean;
+  // TreeSHAP: the root-to-leaf paths of every tree
+  DBuf<PathEl> path_el;      // elements, path after path
+  DBuf<int> path_off;        // [n_paths + 1] element offsets
+  DBuf<float> path_leaf;     // [n_paths] leaf values
+  DBuf<int> tree_path;       // [n_trees + 1] first path of each tree
+  DBuf<int4> shap_chunk;     // {class, first path, end path, -} work units of TreeSHAP blocks
+  int n_shap_chunks = 0;
   int n_trees = 0;
   int max_depth = 0;
+  int max_path_len = 0;      // elements, bias included
 };
 
 }  // namespace sb

@@ -67,6 +67,18 @@ __device__ __forceinline__ float route(const PredDev& P, int t, const float* row
   }
 }
 
+// Margins in two phases. Phase 1 routes every (row, tree) pair in parallel
+// (a thread takes one row through a few consecutive trees) and stores the
+// leaf values tree-major. Phase 2 adds them per (row, class) in tree order
+// with separate f32 multiply and add, which is the reference's accumulation
+// (predict_margin_limited), so margins are bit-identical: a block takes
+// PRED_ROWS rows, stages chunks of PRED_CHUNK trees' leaf values through
+// shared memory with coalesced loads from all its warps, and warp 0 (lane =
+// row) runs the ordered sums.
+constexpr int PRED_ROWS = 32;
+constexpr int PRED_WARPS = 4;
+constexpr int PRED_CHUNK = 128;
+
 __global__ void k_leaf_values(PredDev P, const float* __restrict__ X, size_t n, int F, float missing,
                               int tree_limit, int trees_per_block, float* __restrict__ buf) {
   const bool miss_nan = isnan(missing);
@@ -78,21 +90,65 @@ __global__ void k_leaf_values(PredDev P, const float* __restrict__ X, size_t n, 
   for (int t = t0; t < t1; ++t) buf[(size_t)t * n + r] = route(P, t, row, missing, miss_nan);
 }
 
-__global__ void k_margin_sum(PredDev P, const float* __restrict__ buf, size_t n, int K, int tree_limit,
-                             float base, const float* __restrict__ base_margin, int bm_len_kind,
-                             float* __restrict__ out) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (row, class)
-  if (i >= n * K) return;
-  size_t r = i / K;
-  int c = (int)(i - r * K);
-  float acc = base;
-  if (bm_len_kind == 1) acc = base_margin[i];       // n*K
-  else if (bm_len_kind == 2) acc = base_margin[r];  // n
-  for (int t = c; t < tree_limit; t += K) {
-    float w = P.weights ? P.weights[t] : 1.0f;
-    acc = __fadd_rn(acc, __fmul_rn(w, buf[(size_t)t * n + r]));
+__global__ void __launch_bounds__(PRED_ROWS * PRED_WARPS)
+    k_margin_sum(PredDev P, const float* __restrict__ buf, size_t n, int K, int tree_limit, float base,
+                 const float* __restrict__ base_margin, int bm_kind, float* __restrict__ out) {
+  __shared__ float leaf_s[PRED_CHUNK][PRED_ROWS];
+  __shared__ float acc_s[16][PRED_ROWS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t r = (size_t)blockIdx.x * PRED_ROWS + lane;
+  const bool in = r < n;
+  // the running sums: shared memory for up to 16 classes, else `out` itself
+  const bool in_smem = K <= 16;
+  auto acc = [&](int c) -> float& { return in_smem ? acc_s[c][lane] : out[(in ? r : 0) * K + c]; };
+  if (warp == 0 && (in || in_smem))
+    for (int c = 0; c < K; ++c) {
+      float a = base;
+      if (in && bm_kind == 1) a = base_margin[r * K + c];  // n*K
+      else if (in && bm_kind == 2) a = base_margin[r];     // n
+      acc(c) = a;
+    }
+  for (int t0 = 0; t0 < tree_limit; t0 += PRED_CHUNK) {
+    const int t1 = min(tree_limit, t0 + PRED_CHUNK);
+    for (int t = t0 + warp; t < t1; t += PRED_WARPS) leaf_s[t - t0][lane] = in ? buf[(size_t)t * n + r] : 0.0f;
+    __syncthreads();
+    if (warp == 0 && (in || in_smem)) {
+      if (K == 1) {
+        float a = acc(0);
+        for (int t = t0; t < t1; ++t) {
+          const float w = P.weights ? P.weights[t] : 1.0f;
+          a = __fadd_rn(a, __fmul_rn(w, leaf_s[t - t0][lane]));
+        }
+        acc(0) = a;
+      } else {
+        for (int t = t0; t < t1; ++t) {
+          const float w = P.weights ? P.weights[t] : 1.0f;
+          float& a = acc(t % K);
+          a = __fadd_rn(a, __fmul_rn(w, leaf_s[t - t0][lane]));
+        }
+      }
+    }
+    __syncthreads();
   }
-  out[i] = acc;
+  if (warp == 0 && in && in_smem)
+    for (int c = 0; c < K; ++c) out[r * K + c] = acc_s[c][lane];
+}
+
+// Both phases over n rows, in chunks of `chunk` rows (buf holds chunk * T floats).
+int margins(sb_ctx* ctx, cudaStream_t st, const PredDev& P, const float* d_X, size_t n, size_t F, float missing,
+            int K, int limit, float base, const float* d_bm, int bm_kind, float* d_buf, size_t chunk, float* d_out) {
+  for (size_t r0 = 0; r0 < n; r0 += chunk) {
+    const size_t nb = std::min(chunk, n - r0);
+    if (limit > 0) {
+      const int tpb = nb < 16384 ? 2 : 8;  // small batches: more (row, tree) pairs in flight
+      dim3 grid((unsigned)((nb + 127) / 128), (unsigned)((limit + tpb - 1) / tpb));
+      SB_LAUNCH_ON(ctx, st, k_leaf_values, grid, 128, 0, P, d_X + r0 * F, nb, (int)F, missing, limit, tpb, d_buf);
+    }
+    const float* bm = d_bm ? d_bm + (bm_kind == 1 ? r0 * K : r0) : nullptr;
+    SB_LAUNCH_ON(ctx, st, k_margin_sum, (unsigned)((nb + PRED_ROWS - 1) / PRED_ROWS), PRED_ROWS * PRED_WARPS, 0, P,
+                 d_buf, nb, K, limit, base, bm, bm ? bm_kind : 0, d_out + r0 * K);
+  }
+  return SB_OK;
 }
 
 __global__ void k_transform(float* __restrict__ v, size_t n, int K, int objective) {
@@ -123,132 +179,122 @@ __global__ void k_transform(float* __restrict__ v, size_t n, int K, int objectiv
 }
 
 // ------------------------------------------------------------- TreeSHAP
-struct PE {
-  int f;
-  double z, o, w;
+// Path-dependent TreeSHAP (shap.rs:49-367) restated per root-to-leaf path.
+// At a leaf, the recursive walk's path holds one element per feature split
+// on the way (a repeated feature is unwound and extended again with the
+// products of its fractions), with one-fraction o = [the row follows every
+// such split] and zero-fraction z = the product of their cover fractions. So
+// each leaf's contribution to a row is: EXTEND over its merged elements,
+// then, per element, UNWOUND_SUM times (o - z) times the leaf value. The
+// elements' order does not change the weights.
+//
+// A block takes SHAP_ROWS rows (one per thread) over one chunk of at most
+// SHAP_CHUNK paths of one tree. Each thread adds its row's contributions
+// into a feature-major f32 partial in shared memory (its own column: no
+// conflicts, no atomics), flushed to the f64 accumulator at the end. Blocks
+// stay short (a few hundred microseconds at depth 8) and have the same 128
+// threads as the margin kernels' blocks, so when a TreeSHAP block retires a
+// waiting margin block (on a higher-priority stream) fits in its place.
+constexpr int SHAP_ROWS = 128;
+constexpr int SHAP_CHUNK = 64;  // paths per block
+
+__constant__ double c_inv[32];  // 1 / k
+
+struct ShapPathsDev {
+  const PathEl* el;
+  const int* off;
+  const float* leaf;
+  const int4* chunk;  // {class, first path, end path, -}
 };
 
-__device__ void extend_path(PE* path, int& len, double z, double o, int f) {  // shap.rs:49-68
-  const int ud = len;
-  path[ud].f = f;
-  path[ud].z = z;
-  path[ud].o = o;
-  path[ud].w = ud == 0 ? 1.0 : 0.0;
-  const double denom = (double)(ud + 1);
-  for (int i = ud - 1; i >= 0; --i) {
-    double pw = path[i].w;
-    path[i + 1].w += o * pw * (double)(i + 1) / denom;
-    path[i].w = z * pw * (double)(ud - i) / denom;
-  }
-  len = ud + 1;
-}
-__device__ void unwind_path(PE* path, int& len, int pi) {  // shap.rs:72-94
-  const int ud = len - 1;
-  const double o = path[pi].o, z = path[pi].z;
-  double next = path[ud].w;
-  const double denom = (double)(ud + 1);
-  for (int i = ud - 1; i >= 0; --i) {
-    if (o != 0.0) {
-      double tmp = path[i].w;
-      path[i].w = next * denom / ((double)(i + 1) * o);
-      next = tmp - path[i].w * z * (double)(ud - i) / denom;
-    } else if (z != 0.0) {
-      path[i].w = path[i].w * denom / (z * (double)(ud - i));
-    }
-  }
-  for (int i = pi; i < ud; ++i) {
-    path[i].f = path[i + 1].f;
-    path[i].z = path[i + 1].z;
-    path[i].o = path[i + 1].o;
-  }
-  len = ud;
-}
-__device__ double unwound_path_sum(const PE* path, int len, int pi) {  // shap.rs:98-116
-  const int ud = len - 1;
-  const double o = path[pi].o, z = path[pi].z;
-  double next = path[ud].w;
-  const double denom = (double)(ud + 1);
-  double total = 0.0;
-  for (int i = ud - 1; i >= 0; --i) {
-    if (o != 0.0) {
-      double tmp = next * denom / ((double)(i + 1) * o);
-      total += tmp;
-      next = path[i].w - tmp * z * (double)(ud - i) / denom;
-    } else if (z != 0.0) {
-      total += (path[i].w / z) / ((double)(ud - i) / denom);
-    }
-  }
-  return total;
-}
-
-struct ShapDev {
-  const sb_node* nodes;
-  const int64_t* tree_off;
-  int n_trees;
-};
-
-__global__ void k_shap(ShapDev P, const float* __restrict__ X, size_t n, int F, int K, float missing,
-                       int trees_per_block, double* __restrict__ acc) {
+template <int MAXL>
+__global__ void __launch_bounds__(SHAP_ROWS) k_shap_paths(ShapPathsDev P, const float* __restrict__ X, size_t n,
+                                                         int F, int K, float missing, unsigned row_blocks,
+                                                         double* __restrict__ acc) {
+  extern __shared__ float ph[];          // [F][R] contributions of this block
+  const int R = SHAP_ROWS;
+  const int tid = threadIdx.x;
+  const unsigned rb = blockIdx.x % row_blocks;  // 1-D grid over (path chunk, row block)
+  const size_t r0 = (size_t)rb * R;
+  const int4 ch = P.chunk[blockIdx.x / row_blocks];
+  const int c = ch.x;
+  for (int i = tid; i < F * R; i += R) ph[i] = 0.0f;
+  const float* row = X + (r0 + tid < n ? r0 + tid : r0) * (size_t)F;  // L1-resident while the block runs
+  __syncwarp();
   const bool miss_nan = isnan(missing);
-  size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  const float* row = X + r * F;
-  const int width = F + 1;
-  PE paths[SHAP_MAXD + 2][SHAP_MAXD + 2];
-  int lens[SHAP_MAXD + 2];
-  struct Item {
-    int nid, d, f;
-    double z, o;
-  } stack[2 * SHAP_MAXD + 4];
-  int t0 = blockIdx.y * trees_per_block;
-  int t1 = min(P.n_trees, t0 + trees_per_block);
-  for (int t = t0; t < t1; ++t) {
-    const sb_node* nd = P.nodes + P.tree_off[t];
-    double* phi = acc + (r * K + (t % K)) * (size_t)width;
-    int sp = 0;
-    stack[sp++] = Item{0, 0, -1, 1.0, 1.0};
-    while (sp > 0) {
-      Item it = stack[--sp];
-      PE* path = paths[it.d];
-      int len = 0;
-      if (it.d > 0) {
-        len = lens[it.d - 1];
-        for (int i = 0; i < len; ++i) path[i] = paths[it.d - 1][i];
-      }
-      extend_path(path, len, it.z, it.o, it.f);
-      const sb_node& node = nd[it.nid];
-      const int ud = len - 1;
-      if (node.left < 0) {
-        const double leaf = (double)node.leaf_value;
-        for (int i = 1; i <= ud; ++i) {
-          double w = unwound_path_sum(path, len, i);
-          atomicAdd(&phi[path[i].f], w * (path[i].o - path[i].z) * leaf * 1.0);
+  {
+    for (int p = ch.y; p < ch.z; ++p) {
+      const int e0 = P.off[p], L = P.off[p + 1] - e0;
+      const double leaf = (double)P.leaf[p];
+      double w[MAXL], z[MAXL], iz[MAXL], o[MAXL];
+      int fe[MAXL];
+#pragma unroll
+      for (int e = 0; e < MAXL; ++e) {
+        fe[e] = -1;
+        z[e] = 1.0;
+        iz[e] = 1.0;
+        o[e] = 1.0;
+        if (e < L) {
+          const PathEl el = P.el[e0 + e];
+          fe[e] = el.f;
+          z[e] = el.z;
+          iz[e] = el.inv_z;
+          if (el.f >= 0) {
+            const float v = __ldg(row + el.f);
+            const bool mis = miss_nan ? isnan(v) : v == missing;
+            o[e] = (mis ? el.miss_ok != 0 : (v >= el.lo && v < el.hi)) ? 1.0 : 0.0;
+          }
         }
-        lens[it.d] = len;
-        continue;
       }
-      float v = row[node.split_feature];
-      // the reference routes by `v < split_cond` here, categorical or not
-      bool go_left = is_missing_d(v, missing, miss_nan) ? node.default_left != 0 : v < node.split_cond;
-      int hot = go_left ? node.left : node.right, cold = go_left ? node.right : node.left;
-      double cover = (double)node.sum_hess, hz = 0.0, cz = 0.0;
-      if (cover > 0.0) {
-        hz = (double)nd[hot].sum_hess / cover;
-        cz = (double)nd[cold].sum_hess / cover;
-      }
-      int si = (int)node.split_feature;
-      double iz = 1.0, io = 1.0;
-      for (int i = 1; i <= ud; ++i)
-        if (path[i].f == si) {
-          iz = path[i].z;
-          io = path[i].o;
-          unwind_path(path, len, i);
-          break;
+      // EXTEND (extend_path, shap.rs:49-68) over every element
+      w[0] = 1.0;
+#pragma unroll
+      for (int e = 1; e < MAXL; ++e) {
+        w[e] = 0.0;
+        if (e < L) {
+          const double inv = c_inv[e + 1];
+#pragma unroll
+          for (int i = e - 1; i >= 0; --i) {
+            const double pw = w[i];
+            w[i + 1] += o[e] * pw * (double)(i + 1) * inv;
+            w[i] = z[e] * pw * (double)(e - i) * inv;
+          }
         }
-      lens[it.d] = len;
-      if (it.d + 1 > SHAP_MAXD) continue;  // guarded by the host (depth check)
-      stack[sp++] = Item{cold, it.d + 1, si, cz * iz, 0.0};
-      stack[sp++] = Item{hot, it.d + 1, si, hz * iz, io};
+      }
+      const int ud = L - 1;
+      double wl = 0.0;
+#pragma unroll
+      for (int e = 0; e < MAXL; ++e)
+        if (e == ud) wl = w[e];
+      const double dn = (double)(ud + 1), idn = c_inv[ud + 1];
+      // UNWOUND_SUM (unwound_path_sum, shap.rs:98-116) per element
+#pragma unroll
+      for (int e = 1; e < MAXL; ++e) {
+        if (e < L) {
+          const double oo = o[e], zz = z[e];
+          double next = wl, total = 0.0;
+#pragma unroll
+          for (int i = MAXL - 2; i >= 0; --i) {
+            if (i < ud) {
+              if (oo != 0.0) {
+                const double tmp = next * dn * c_inv[i + 1];
+                total += tmp;
+                next = w[i] - tmp * zz * (double)(ud - i) * idn;
+              } else if (zz != 0.0) {
+                total += w[i] * iz[e] * dn * c_inv[ud - i];
+              }
+            }
+          }
+          ph[fe[e] * R + tid] += (float)(total * (oo - zz) * leaf);
+        }
+      }
+    }
+  }
+  if (r0 + tid < n) {
+    double* a = acc + ((r0 + tid) * K + c) * (size_t)(F + 1);
+    for (int f = 0; f < F; ++f) {
+      const float v = ph[f * R + tid];
+      if (v != 0.0f) atomicAdd(a + f, (double)v);
     }
   }
 }
@@ -299,7 +345,6 @@ int model_upload(sb_model* m) {
   for (int t = 0; t < T; ++t) off[t + 1] = off[t] + (int64_t)m->trees[t].nodes.size();
   std::vector<int4> packed(off[T]);
   std::vector<int> catend(off[T], 0);
-  std::vector<sb_node> full(off[T]);
   std::vector<uint32_t> cats;
   int maxd = 0;
   for (int t = 0; t < T; ++t) {
@@ -326,19 +371,16 @@ int model_upload(sb_model* m) {
       x.z = nd.left;
       x.w = nd.right;
       packed[off[t] + i] = x;
-      full[off[t] + i] = nd;
     }
     maxd = std::max(maxd, tree_depth(tr));
   }
   SB_TRY(D.nodes.alloc(ctx, std::max<size_t>(packed.size(), 1)));
-  SB_TRY(D.full.alloc(ctx, std::max<size_t>(full.size(), 1)));
   SB_TRY(D.tree_off.alloc(ctx, T + 1));
   SB_TRY(D.cats.alloc(ctx, std::max<size_t>(cats.size(), 1)));
   SB_TRY(D.weights.alloc(ctx, std::max(T, 1)));
   cudaStream_t st = ctx->stream;
   if (!packed.empty()) {
     SB_CUDA(cudaMemcpyAsync(D.nodes.p, packed.data(), packed.size() * 16, cudaMemcpyHostToDevice, st));
-    SB_CUDA(cudaMemcpyAsync(D.full.p, full.data(), full.size() * sizeof(sb_node), cudaMemcpyHostToDevice, st));
   }
   SB_CUDA(cudaMemcpyAsync(D.tree_off.p, off.data(), (T + 1) * 8, cudaMemcpyHostToDevice, st));
   if (!cats.empty()) SB_CUDA(cudaMemcpyAsync(D.cats.p, cats.data(), cats.size() * 4, cudaMemcpyHostToDevice, st));
@@ -348,6 +390,86 @@ int model_upload(sb_model* m) {
     SB_CUDA(cudaMemcpyAsync(D.cat_end.p, catend.data(), catend.size() * 4, cudaMemcpyHostToDevice, st));
   std::vector<double> means(T);
   for (int t = 0; t < T; ++t) means[t] = node_mean_value(m->trees[t], 0);
+  // TreeSHAP paths: per leaf, its merged path elements
+  std::vector<PathEl> pel;
+  std::vector<int> poff(1, 0), tpath(1, 0);
+  std::vector<float> pleaf;
+  int maxlen = 1;
+  for (int t = 0; t < T; ++t) {
+    const HostTree& tr = m->trees[t];
+    struct Frame {
+      int nid;
+      std::vector<PathEl> el;
+    };
+    std::vector<Frame> stack;
+    PathEl bias{-1, 1, -INFINITY, INFINITY, 1.0, 1.0};
+    stack.push_back(Frame{0, {bias}});
+    while (!stack.empty() && !tr.nodes.empty()) {
+      Frame fr = std::move(stack.back());
+      stack.pop_back();
+      const sb_node& nd = tr.nodes[fr.nid];
+      if (nd.left < 0) {
+        for (PathEl& e : fr.el) e.inv_z = e.z != 0.0 ? 1.0 / e.z : 0.0;
+        pel.insert(pel.end(), fr.el.begin(), fr.el.end());
+        poff.push_back((int)pel.size());
+        pleaf.push_back(nd.leaf_value);
+        maxlen = std::max(maxlen, (int)fr.el.size());
+        continue;
+      }
+      const double cover = (double)nd.sum_hess;
+      for (int side = 0; side < 2; ++side) {
+        const int child = side == 0 ? nd.left : nd.right;
+        const double zf = cover > 0.0 ? (double)tr.nodes[child].sum_hess / cover : 0.0;
+        Frame nx{child, fr.el};
+        size_t e = 1;
+        while (e < nx.el.size() && nx.el[e].f != (int)nd.split_feature) ++e;
+        if (e == nx.el.size()) nx.el.push_back(PathEl{(int)nd.split_feature, 1, -INFINITY, INFINITY, 1.0, 1.0});
+        PathEl& el = nx.el[e];
+        el.z *= zf;  // cover fraction of this split, times the earlier ones
+        if (side == 0) {  // v < cond, or missing when default_left
+          el.hi = std::min(el.hi, nd.split_cond);
+          el.miss_ok = el.miss_ok && nd.default_left;
+        } else {
+          el.lo = std::max(el.lo, nd.split_cond);
+          el.miss_ok = el.miss_ok && !nd.default_left;
+        }
+        stack.push_back(std::move(nx));
+      }
+    }
+    tpath.push_back((int)pleaf.size());
+  }
+  SB_TRY(D.path_el.alloc(ctx, std::max<size_t>(pel.size(), 1)));
+  SB_TRY(D.path_off.alloc(ctx, poff.size()));
+  SB_TRY(D.path_leaf.alloc(ctx, std::max<size_t>(pleaf.size(), 1)));
+  SB_TRY(D.tree_path.alloc(ctx, tpath.size()));
+  if (!pel.empty())
+    SB_CUDA(cudaMemcpyAsync(D.path_el.p, pel.data(), pel.size() * sizeof(PathEl), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(D.path_off.p, poff.data(), poff.size() * 4, cudaMemcpyHostToDevice, st));
+  if (!pleaf.empty())
+    SB_CUDA(cudaMemcpyAsync(D.path_leaf.p, pleaf.data(), pleaf.size() * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(D.tree_path.p, tpath.data(), tpath.size() * 4, cudaMemcpyHostToDevice, st));
+  std::vector<int4> chunks;  // <= SHAP_CHUNK paths of one tree each
+  const int Kc = m->num_class >= 2 ? m->num_class : 1;
+  for (int t = 0; t < T; ++t)
+    for (int p0 = tpath[t]; p0 < tpath[t + 1]; p0 += SHAP_CHUNK)
+      chunks.push_back(make_int4(t % Kc, p0, std::min(p0 + SHAP_CHUNK, tpath[t + 1]), 0));
+  SB_TRY(D.shap_chunk.alloc(ctx, std::max<size_t>(chunks.size(), 1)));
+  if (!chunks.empty())
+    SB_CUDA(cudaMemcpyAsync(D.shap_chunk.p, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  D.n_shap_chunks = (int)chunks.size();
+  {  // shared memory of the TreeSHAP blocks: f32 partials of SHAP_ROWS rows
+    const int smem = (int)std::min<size_t>((size_t)m->n_features * SHAP_ROWS * 4, ctx->smem_optin);
+    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<SHAP_MAXD + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  }
+  D.max_path_len = maxlen;
+  {
+    double inv[32];
+    inv[0] = 0.0;
+    for (int k = 1; k < 32; ++k) inv[k] = 1.0 / (double)k;
+    SB_CUDA(cudaMemcpyToSymbolAsync(c_inv, inv, sizeof(inv), 0, cudaMemcpyHostToDevice, st));
+  }
   SB_TRY(D.tree_mean.alloc(ctx, std::max(T, 1)));
   if (T) SB_CUDA(cudaMemcpyAsync(D.tree_mean.p, means.data(), T * 8, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaStreamSynchronize(st));
@@ -355,6 +477,12 @@ int model_upload(sb_model* m) {
   D.max_depth = maxd;
   m->dev_valid = true;
   return SB_OK;
+}
+
+// Rows per phase-1 chunk, so that the tree-major leaf buffer stays <= 64 MB.
+size_t margin_chunk_rows(const sb_model* m) {
+  const size_t T = (size_t)std::max(m->dev.n_trees, 1);
+  return std::max<size_t>(1024, (size_t)(64ull << 20) / (T * 4));
 }
 
 int predict_margin_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing,
@@ -371,23 +499,46 @@ int predict_margin_device(sb_model* m, const float* d_X, size_t n, size_t F, flo
   P.cats = m->dev.cats.p;
   P.weights = m->dev.weights.p;
   P.n_trees = T;
-  // rows per batch so the tree-major leaf buffer stays <= 256 MB
-  size_t batch = limit > 0 ? std::max<size_t>(1024, (size_t)(64ull << 20) / (size_t)limit) : n;
-  batch = std::min(batch, n);
+  if (n == 0) return SB_OK;
+  const size_t chunk = std::min(n, margin_chunk_rows(m));  // leaf buffer <= 64 MB
   DBuf<float> buf;
-  if (limit > 0) SB_TRY(buf.alloc(ctx, (size_t)limit * std::max<size_t>(batch, 1)));
-  for (size_t r0 = 0; r0 < n; r0 += batch) {
-    size_t nb = std::min(batch, n - r0);
-    if (limit > 0) {
-      const int tpb = 8;
-      dim3 grid((unsigned)((nb + 127) / 128), (unsigned)((limit + tpb - 1) / tpb));
-      SB_LAUNCH(ctx, k_leaf_values, grid, 128, 0, P, d_X + r0 * F, nb, (int)F, missing, limit, tpb, buf.p);
-    }
-    const float* bm = d_base_margin ? d_base_margin + (bm_kind == 1 ? r0 * Kc : r0) : nullptr;
-    size_t tot = nb * Kc;
-    SB_LAUNCH(ctx, k_margin_sum, (unsigned)((tot + 255) / 256), 256, 0, P, buf.p, nb, Kc, limit,
-              m->base_score, bm, bm ? bm_kind : 0, d_out + r0 * Kc);
-  }
+  if (limit > 0) SB_TRY(buf.alloc(ctx, (size_t)limit * chunk));
+  return margins(ctx, ctx->stream, P, d_X, n, F, missing, Kc, limit, m->base_score, d_base_margin, bm_kind, buf.p,
+                 chunk, d_out);
+}
+
+// TreeSHAP contributions of n rows into d_acc ([n][K][F+1] doubles, zeroed
+// here) on stream st.
+int shap_paths(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t F, float missing,
+               double* d_acc) {
+  sb_ctx* ctx = m->ctx;
+  SB_REQUIRE(m->dev.max_depth <= SHAP_MAXD, SB_ERR_UNSUPPORTED,
+             "TreeSHAP on the device supports trees up to depth %d (got %d)", SHAP_MAXD, m->dev.max_depth);
+  const int K = m->num_class >= 2 ? m->num_class : 1;
+  const int T = m->dev.n_trees;
+  SB_CUDA(cudaMemsetAsync(d_acc, 0, n * K * (F + 1) * sizeof(double), st));
+  if (T == 0 || n == 0) return SB_OK;
+  const int R = SHAP_ROWS;
+  const size_t smem = (size_t)F * R * 4;
+  SB_REQUIRE(smem <= ctx->smem_optin, SB_ERR_UNSUPPORTED, "TreeSHAP on the device supports up to %zu features",
+             ctx->smem_optin / (4 * R));
+  ShapPathsDev P;
+  P.el = m->dev.path_el.p;
+  P.off = m->dev.path_off.p;
+  P.leaf = m->dev.path_leaf.p;
+  P.chunk = m->dev.shap_chunk.p;
+  const unsigned row_blocks = (unsigned)((n + R - 1) / R);
+  SB_REQUIRE((uint64_t)row_blocks * m->dev.n_shap_chunks < (1ull << 31), SB_ERR_UNSUPPORTED,
+             "TreeSHAP of %zu rows over %d path chunks exceeds one launch", n, m->dev.n_shap_chunks);
+  const unsigned grid = row_blocks * (unsigned)m->dev.n_shap_chunks;
+  const int L = m->dev.max_path_len;
+  if (L <= 5)
+    SB_LAUNCH_ON(ctx, st, k_shap_paths<5>, grid, R, smem, P, d_X, n, (int)F, K, missing, row_blocks, d_acc);
+  else if (L <= 9)
+    SB_LAUNCH_ON(ctx, st, k_shap_paths<9>, grid, R, smem, P, d_X, n, (int)F, K, missing, row_blocks, d_acc);
+  else
+    SB_LAUNCH_ON(ctx, st, k_shap_paths<SHAP_MAXD + 1>, grid, R, smem, P, d_X, n, (int)F, K, missing, row_blocks,
+                 d_acc);
   return SB_OK;
 }
 
@@ -395,8 +546,6 @@ int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, f
                             float* d_out) {
   sb_ctx* ctx = m->ctx;
   SB_TRY(model_upload(m));
-  SB_REQUIRE(m->dev.max_depth <= SHAP_MAXD, SB_ERR_UNSUPPORTED,
-             "TreeSHAP on the device supports trees up to depth %d (got %d)", SHAP_MAXD, m->dev.max_depth);
   const int K = m->num_class >= 2 ? m->num_class : 1;
   const int T = m->dev.n_trees;
   const size_t width = F + 1;
@@ -412,17 +561,8 @@ int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, f
   DBuf<double> d_bias, acc;
   SB_TRY(d_bias.alloc(ctx, K));
   SB_CUDA(cudaMemcpyAsync(d_bias.p, bias.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
-  SB_TRY(acc.alloc(ctx, n * K * width));
-  SB_CUDA(cudaMemsetAsync(acc.p, 0, acc.bytes(), ctx->stream));
-  ShapDev P;
-  P.nodes = m->dev.full.p;
-  P.tree_off = m->dev.tree_off.p;
-  P.n_trees = T;
-  if (T > 0 && n > 0) {
-    const int tpb = 4;
-    dim3 grid((unsigned)((n + 63) / 64), (unsigned)((T + tpb - 1) / tpb));
-    SB_LAUNCH(ctx, k_shap, grid, 64, 0, P, d_X, n, (int)F, K, missing, tpb, acc.p);
-  }
+  SB_TRY(acc.alloc(ctx, std::max<size_t>(n * K * width, 1)));
+  SB_TRY(shap_paths(m, ctx->stream, d_X, n, F, missing, acc.p));
   size_t tot = n * K * width;
   if (tot) SB_LAUNCH(ctx, k_shap_finish, (unsigned)((tot + 255) / 256), 256, 0, acc.p, d_bias.p, n, K, (int)F, d_out);
   return SB_OK;
@@ -431,35 +571,20 @@ int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, f
 // ---- batch launchers on an explicit stream with caller-owned buffers (used
 // by the serving loop; the model must be resident, see model_upload)
 
-size_t margin_chunk_rows(const sb_model* m) {
-  const size_t T = (size_t)std::max(m->dev.n_trees, 1);
-  return std::max<size_t>(1024, (size_t)(64ull << 20) / (T * 4));  // leaf buffer <= 64 MB
-}
-
 int margin_batch(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t F, float missing,
                  float* d_buf, size_t buf_rows, float* d_out) {
   sb_ctx* ctx = m->ctx;
   const int Kc = m->num_class >= 2 ? m->num_class : 1;
-  const int T = m->dev.n_trees;
   PredDev P;
   P.nodes = m->dev.nodes.p;
   P.cat_end = m->dev.cat_end.p;
   P.tree_off = m->dev.tree_off.p;
   P.cats = m->dev.cats.p;
   P.weights = m->dev.weights.p;
-  P.n_trees = T;
-  for (size_t r0 = 0; r0 < n; r0 += buf_rows) {
-    const size_t nb = std::min(buf_rows, n - r0);
-    if (T > 0) {
-      const int tpb = 8;
-      dim3 grid((unsigned)((nb + 127) / 128), (unsigned)((T + tpb - 1) / tpb));
-      SB_LAUNCH_ON(ctx, st, k_leaf_values, grid, 128, 0, P, d_X + r0 * F, nb, (int)F, missing, T, tpb, d_buf);
-    }
-    const size_t tot = nb * Kc;
-    SB_LAUNCH_ON(ctx, st, k_margin_sum, (unsigned)((tot + 255) / 256), 256, 0, P, d_buf, nb, Kc, T,
-                 m->base_score, (const float*)nullptr, 0, d_out + r0 * Kc);
-  }
-  return SB_OK;
+  P.n_trees = m->dev.n_trees;
+  if (n == 0) return SB_OK;
+  return margins(ctx, st, P, d_X, n, F, missing, Kc, m->dev.n_trees, m->base_score, nullptr, 0, d_buf, buf_rows,
+                 d_out);
 }
 
 int contribs_bias(sb_model* m, std::vector<double>* bias) {
@@ -473,21 +598,9 @@ int contribs_bias(sb_model* m, std::vector<double>* bias) {
 int contribs_batch(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t F, float missing,
                    double* d_acc, const double* d_bias, float* d_out) {
   sb_ctx* ctx = m->ctx;
-  SB_REQUIRE(m->dev.max_depth <= SHAP_MAXD, SB_ERR_UNSUPPORTED,
-             "TreeSHAP on the device supports trees up to depth %d (got %d)", SHAP_MAXD, m->dev.max_depth);
   const int K = m->num_class >= 2 ? m->num_class : 1;
-  const int T = m->dev.n_trees;
   const size_t tot = n * K * (F + 1);
-  SB_CUDA(cudaMemsetAsync(d_acc, 0, tot * sizeof(double), st));
-  ShapDev P;
-  P.nodes = m->dev.full.p;
-  P.tree_off = m->dev.tree_off.p;
-  P.n_trees = T;
-  if (T > 0 && n > 0) {
-    const int tpb = 4;
-    dim3 grid((unsigned)((n + 63) / 64), (unsigned)((T + tpb - 1) / tpb));
-    SB_LAUNCH_ON(ctx, st, k_shap, grid, 64, 0, P, d_X, n, (int)F, K, missing, tpb, d_acc);
-  }
+  SB_TRY(shap_paths(m, st, d_X, n, F, missing, d_acc));
   if (tot) SB_LAUNCH_ON(ctx, st, k_shap_finish, (unsigned)((tot + 255) / 256), 256, 0, d_acc, d_bias, n, K, (int)F, d_out);
   return SB_OK;
 }

@@ -3,19 +3,20 @@
 // (predict_contribs, learner/shap.rs:321-367) requests with continuous
 // batching.
 //
-//   submit  : any thread; the request joins a FIFO queue.
-//   dispatcher thread : whenever a slot (a pair of CUDA streams) is free, it
-//             takes the longest run of queued requests at the head of the
-//             queue that share a kind and a missing-value marker, up to a row
-//             cap, and admits it if its device buffers fit in the free part of
-//             the loop's memory budget (first-fit arena); otherwise the head
-//             waits until a finishing batch frees memory. The batch's rows are
-//             copied into one device buffer, run as one set of kernel launches
-//             and copied back per request. Margin batches run on
-//             high-priority streams and TreeSHAP batches on low-priority ones,
-//             so heavy attribution work does not hold up margins. Several
+//   submit  : any thread; the request joins its kind's FIFO queue.
+//   dispatcher thread : each kind has its own slots (a slot is a CUDA
+//             stream: high priority for margins, low for TreeSHAP). Whenever
+//             a slot is free, the dispatcher takes the longest run at the
+//             head of that kind's queue sharing a missing-value marker, up to
+//             a row cap, and admits it if its device buffers fit in the free
+//             part of the loop's memory budget (first-fit arena); otherwise
+//             that queue's head waits until a finishing batch frees memory.
+//             The batch's rows are copied into one device buffer, run as one
+//             set of kernel launches and copied back per request. Several
 //             batches are in flight at once, so requests that arrive while
-//             others are on the GPU are admitted as slots and memory free up.
+//             others are on the GPU are admitted as slots and memory free up;
+//             heavy TreeSHAP work never takes a margin slot, and its short
+//             kernel blocks give margin kernels SMs as soon as they arrive.
 //   completion : a host function queued behind each batch flags the slot; the
 //             dispatcher then marks the requests done and frees their memory.
 //
@@ -47,7 +48,7 @@ struct Server;
 namespace {
 
 constexpr size_t ALIGN = 256;
-constexpr size_t MARGIN_BATCH_ROWS = 131072;   // row cap of one margin batch
+constexpr size_t MARGIN_BATCH_ROWS = 65536;    // row cap of one margin batch
 constexpr size_t CONTRIBS_BATCH_ROWS = 65536;  // row cap of one TreeSHAP batch
 
 double now_s() {
@@ -115,7 +116,8 @@ struct Arena {
 
 struct Slot {
   Server* srv = nullptr;
-  cudaStream_t hi = nullptr, lo = nullptr;
+  cudaStream_t st = nullptr;
+  int kind = 0;
   bool busy = false;
   bool finished = false;  // set by the completion host function (under the mutex)
   std::vector<std::shared_ptr<Request>> reqs;
@@ -129,7 +131,7 @@ struct Server {
   sb_ctx* ctx = nullptr;
   sb_model* model = nullptr;
   int F = 0, K = 1, T = 0;
-  size_t chunk_rows = 0;
+  size_t chunk_rows = 0;  // rows per margin leaf-buffer chunk
   char* d_mem = nullptr;
   double* d_bias = nullptr;
   Arena arena;
@@ -137,11 +139,11 @@ struct Server {
   std::mutex mu;
   std::condition_variable cv;       // dispatcher wake-ups
   std::condition_variable done_cv;  // request completions
-  std::deque<std::shared_ptr<Request>> queue;
+  std::deque<std::shared_ptr<Request>> queue[2];  // per kind
   std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
   uint64_t next_ticket = 1;
   bool stop = false;
-  bool mem_blocked = false;  // the queue head waits for memory to be freed
+  bool mem_blocked[2] = {false, false};  // a queue head waits for memory to be freed
   std::thread worker;
   sb_server_stats stats{};
 
@@ -151,8 +153,8 @@ struct Server {
   // device bytes of a batch of `rows` rows
   size_t batch_bytes(int kind, size_t rows) const {
     size_t b = up(rows * F * 4) + up(out_floats(kind, rows) * 4);
-    if (kind == SB_REQ_MARGIN) b += up(std::min(rows, chunk_rows) * (size_t)std::max(T, 1) * 4);
-    else b += up(out_floats(kind, rows) * 8);
+    if (kind == SB_REQ_MARGIN) b += up(std::min(rows, chunk_rows) * (size_t)std::max(T, 1) * 4);  // leaf values
+    else b += up(out_floats(kind, rows) * 8);  // f64 accumulator
     return b;
   }
 
@@ -170,7 +172,7 @@ struct Server {
     float* dX = reinterpret_cast<float*>(base);
     float* dOut = reinterpret_cast<float*>(base + up(rows * F * 4));
     char* scratch = base + up(rows * F * 4) + up(out_floats(kind, rows) * 4);
-    cudaStream_t st = kind == SB_REQ_MARGIN ? s->hi : s->lo;
+    cudaStream_t st = s->st;
     size_t r0 = 0;
     for (auto& r : s->reqs) {
       SB_CUDA(cudaMemcpyAsync(dX + r0 * F, r->X, r->n * F * 4, cudaMemcpyHostToDevice, st));
@@ -204,21 +206,21 @@ struct Server {
     s->busy = false;
     s->finished = false;
     arena.release(s->mem_off, s->mem_bytes);
-    mem_blocked = false;
+    mem_blocked[0] = mem_blocked[1] = false;
     done_cv.notify_all();
   }
 
   // Takes the longest admissible run at the head of the queue into slot s.
   // Returns the run's rows, 0 when the head must wait for memory.
-  size_t admit(Slot* s, int* kind_out, float* miss_out) {
-    const int kind = queue.front()->kind;
+  size_t admit(Slot* s, int kind, float* miss_out) {
+    std::deque<std::shared_ptr<Request>>& queue = this->queue[kind];
     const float miss = queue.front()->missing;
     const bool miss_nan = std::isnan(miss);
     const size_t cap = kind == SB_REQ_MARGIN ? MARGIN_BATCH_ROWS : CONTRIBS_BATCH_ROWS;
     size_t rows = 0, take = 0;
     for (auto& r : queue) {
       const bool same_miss = miss_nan ? std::isnan(r->missing) : r->missing == miss;
-      if (r->kind != kind || !same_miss) break;
+      if (!same_miss) break;
       if (take > 0 && rows + r->n > cap) break;
       rows += r->n;
       take++;
@@ -241,9 +243,18 @@ struct Server {
     stats.rows += rows;
     stats.max_batch_requests = std::max<uint64_t>(stats.max_batch_requests, take);
     stats.mem_peak = std::max<uint64_t>(stats.mem_peak, arena.used);
-    *kind_out = kind;
     *miss_out = miss;
     return rows;
+  }
+
+  Slot* free_slot(int kind) {
+    for (auto& s : slots)
+      if (s->kind == kind && !s->busy) return s.get();
+    return nullptr;
+  }
+
+  bool can_admit(int kind) {
+    return !queue[kind].empty() && !mem_blocked[kind] && free_slot(kind) != nullptr;
   }
 
   void run() {
@@ -252,46 +263,39 @@ struct Server {
     for (;;) {
       for (auto& s : slots)
         if (s->busy && s->finished) finish(s.get());
-      while (!queue.empty() && !mem_blocked) {
-        Slot* slot = nullptr;
-        for (auto& s : slots)
-          if (!s->busy) {
-            slot = s.get();
+      for (int kind = 0; kind < 2; ++kind) {
+        std::deque<std::shared_ptr<Request>>& queue = this->queue[kind];
+        while (can_admit(kind)) {
+          Slot* slot = free_slot(kind);
+          if (batch_bytes(kind, queue.front()->n) > arena.size) {  // can never fit
+            auto r = queue.front();
+            queue.pop_front();
+            r->status = SB_ERR_OOM;
+            r->done = true;
+            r->t_done = now_s();
+            stats.completed++;
+            stats.failed++;
+            done_cv.notify_all();
+            continue;
+          }
+          float miss = NAN;
+          const size_t rows = admit(slot, kind, &miss);
+          if (rows == 0) {  // the head waits until a finishing batch frees memory
+            mem_blocked[kind] = true;
+            stats.memory_waits++;
             break;
           }
-        if (!slot) break;
-        if (batch_bytes(queue.front()->kind, queue.front()->n) > arena.size) {  // can never fit
-          auto r = queue.front();
-          queue.pop_front();
-          r->status = SB_ERR_OOM;
-          r->done = true;
-          r->t_done = now_s();
-          stats.completed++;
-          stats.failed++;
-          done_cv.notify_all();
-          continue;
+          lk.unlock();
+          const int st = launch(slot, kind, miss, rows);
+          if (st != SB_OK) cudaStreamSynchronize(slot->st);  // let anything already queued drain
+          lk.lock();
+          slot->status = st;
+          if (st != SB_OK) finish(slot);
         }
-        int kind = 0;
-        float miss = NAN;
-        const size_t rows = admit(slot, &kind, &miss);
-        if (rows == 0) {  // the head waits until a finishing batch frees memory
-          mem_blocked = true;
-          stats.memory_waits++;
-          break;
-        }
-        lk.unlock();
-        const int st = launch(slot, kind, miss, rows);
-        if (st != SB_OK) {  // let anything already queued on the slot drain first
-          cudaStreamSynchronize(slot->hi);
-          cudaStreamSynchronize(slot->lo);
-        }
-        lk.lock();
-        slot->status = st;
-        if (st != SB_OK) finish(slot);
       }
       bool any_busy = false;
       for (auto& s : slots) any_busy = any_busy || s->busy;
-      if (stop && queue.empty() && !any_busy) break;
+      if (stop && queue[0].empty() && queue[1].empty() && !any_busy) break;
       // sleep (releasing the mutex, which the completion host functions
       // need) until a batch finishes, a queued request can be admitted, or
       // the loop may stop
@@ -301,11 +305,8 @@ struct Server {
           if (s->busy && s->finished) return true;
           busy = busy || s->busy;
         }
-        if (queue.empty()) return stop && !busy;
-        if (mem_blocked) return false;
-        for (auto& s : slots)
-          if (!s->busy) return true;
-        return false;
+        if (can_admit(0) || can_admit(1)) return true;
+        return stop && queue[0].empty() && queue[1].empty() && !busy;
       });
     }
   }
@@ -356,11 +357,13 @@ int sb_server_create(sb_ctx* ctx, sb_model* m, size_t mem_bytes, int n_slots, sb
   s->arena.init(s->d_mem, mem_bytes);
   int lo_prio = 0, hi_prio = 0;
   SB_CUDA(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
-  for (int i = 0; i < n_slots; ++i) {
+  const int n_shap = std::max(1, n_slots / 2);
+  for (int i = 0; i < n_slots + n_shap; ++i) {  // margin slots, then TreeSHAP slots
     std::unique_ptr<Slot> sl(new Slot);
     sl->srv = s.get();
-    SB_CUDA(cudaStreamCreateWithPriority(&sl->hi, cudaStreamNonBlocking, hi_prio));
-    SB_CUDA(cudaStreamCreateWithPriority(&sl->lo, cudaStreamNonBlocking, lo_prio));
+    sl->kind = i < n_slots ? SB_REQ_MARGIN : SB_REQ_CONTRIBS;
+    SB_CUDA(cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking,
+                                         sl->kind == SB_REQ_MARGIN ? hi_prio : lo_prio));
     s->slots.push_back(std::move(sl));
   }
   s->stats.mem_bytes = mem_bytes;
@@ -394,7 +397,7 @@ int sb_server_submit(sb_server* s, int kind, const float* X, size_t n_rows, size
       r->t_done = r->t_submit;
       s->stats.completed++;
     } else {
-      s->queue.push_back(r);
+      s->queue[kind].push_back(r);
     }
     *ticket = r->ticket;
   }
@@ -438,10 +441,8 @@ int sb_server_destroy(sb_server* s) {
   s->cv.notify_all();
   if (s->worker.joinable()) s->worker.join();
   cudaSetDevice(s->ctx->device);
-  for (auto& sl : s->slots) {
-    if (sl->hi) cudaStreamSynchronize(sl->hi), cudaStreamDestroy(sl->hi);
-    if (sl->lo) cudaStreamSynchronize(sl->lo), cudaStreamDestroy(sl->lo);
-  }
+  for (auto& sl : s->slots)
+    if (sl->st) cudaStreamSynchronize(sl->st), cudaStreamDestroy(sl->st);
   if (s->d_mem) cudaFree(s->d_mem);
   if (s->d_bias) cudaFree(s->d_bias);
   delete s;

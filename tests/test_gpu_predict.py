@@ -85,3 +85,33 @@ def test_dimension_mismatch(sb, ctx, orc):
     m = sb.BoostedModel.from_arrays(*arrays[:4], base, 0, 6, ctx=ctx)
     with pytest.raises(sb.SbError):
         m.predict_margin(sb.DMatrix(x[:, :5]))
+
+
+def test_margins_bit_exact_many_classes_and_trees(sb, ctx, orc):
+    """More than 16 classes (the running sums leave shared memory) and more
+    trees than one chunk of the prediction kernel: random stumps and depth-2
+    trees, against the oracle's sequential sum."""
+    from sequoia_boost_b200.api import NODE_DTYPE
+    rng = np.random.default_rng(17)
+    K, rounds, f = 20, 15, 6  # 300 trees
+    trees = []
+    for t in range(K * rounds):
+        nd = np.zeros(3, NODE_DTYPE)
+        nd["left"] = [1, -1, -1]
+        nd["right"] = [2, -1, -1]
+        nd["split_feature"][0] = rng.integers(0, f)
+        nd["split_cond"][0] = rng.standard_normal()
+        nd["default_left"][0] = rng.integers(0, 2)
+        nd["leaf_value"][1:] = rng.standard_normal(2).astype(np.float32) * 0.1
+        nd["sum_hess"] = [10.0, 4.0, 6.0]
+        trees.append(nd)
+    nodes = np.concatenate(trees)
+    off = np.arange(0, 3 * len(trees) + 1, 3, dtype=np.int64)
+    coff = np.zeros(len(trees) + 1, np.int64)
+    cats = np.zeros(1, np.uint32)
+    arrays = (off, nodes, coff, cats)
+    m = sb.BoostedModel.from_arrays(off, nodes, coff, cats, 0.25, K, f, objective="multi:softprob", ctx=ctx)
+    x, _ = mixed_data(777, f, seed=18)
+    got = m.predict_margin(sb.DMatrix(x))
+    want = orc.predict_margin(arrays, x, 0.25, K)
+    assert np.array_equal(got, want)
