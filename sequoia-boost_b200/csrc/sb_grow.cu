@@ -1750,77 +1750,77 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   const size_t KN = (size_t)K * b->maxn;
   const size_t HB = g->total_bins + g->F;
   cudaStream_t st = ctx->stream;
-  SB_TRY(b->d_mono.alloc(ctx, F));
-  SB_TRY(b->d_in_group.alloc(ctx, F));
-  SB_TRY(b->d_iset.alloc(ctx, (size_t)F * FW));
+  SB_TRY(b->d_mono.alloc_zero(ctx, F));
+  SB_TRY(b->d_in_group.alloc_zero(ctx, F));
+  SB_TRY(b->d_iset.alloc_zero(ctx, (size_t)F * FW));
   SB_CUDA(cudaMemcpyAsync(b->d_mono.p, mono_full.data(), F, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(b->d_in_group.p, in_group.data(), F, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(b->d_iset.p, iset.data(), iset.size() * 4, cudaMemcpyHostToDevice, st));
-  SB_TRY(b->d_round.alloc(ctx, 1));
+  SB_TRY(b->d_round.alloc_zero(ctx, 1));
   SB_CUDA(cudaMemsetAsync(b->d_round.p, 0, 8, st));
-  SB_TRY(b->d_stats.alloc(ctx, KN));
-  SB_TRY(b->d_bounds.alloc(ctx, KN));
-  SB_TRY(b->d_allowed.alloc(ctx, KN * FW));
-  SB_TRY(b->d_fmask.alloc(ctx, KN * FW));
-  SB_TRY(b->d_allowed_all.alloc(ctx, KN));
-  SB_TRY(b->d_built.alloc(ctx, KN));
-  SB_TRY(b->d_seg.alloc(ctx, KN));
-  SB_TRY(b->d_nsamp.alloc(ctx, KN));
-  SB_TRY(b->d_parent.alloc(ctx, KN));
-  SB_TRY(b->d_split.alloc(ctx, KN));
+  SB_TRY(b->d_stats.alloc_zero(ctx, KN));
+  SB_TRY(b->d_bounds.alloc_zero(ctx, KN));
+  SB_TRY(b->d_allowed.alloc_zero(ctx, KN * FW));
+  SB_TRY(b->d_fmask.alloc_zero(ctx, KN * FW));
+  SB_TRY(b->d_allowed_all.alloc_zero(ctx, KN));
+  SB_TRY(b->d_built.alloc_zero(ctx, KN));
+  SB_TRY(b->d_seg.alloc_zero(ctx, KN));
+  SB_TRY(b->d_nsamp.alloc_zero(ctx, KN));
+  SB_TRY(b->d_parent.alloc_zero(ctx, KN));
+  SB_TRY(b->d_split.alloc_zero(ctx, KN));
   SB_CUDA(cudaMemsetAsync(b->d_split.p, 0, b->d_split.bytes(), st));
-  SB_TRY(b->d_leafval.alloc(ctx, KN));
-  SB_TRY(b->d_fill.alloc(ctx, KN));
-  SB_TRY(b->d_lvl.alloc(ctx, 6 * K));
-  SB_TRY(b->d_rows0.alloc(ctx, (size_t)K * b->n));
-  SB_TRY(b->d_rows1.alloc(ctx, (size_t)K * b->n));
-  SB_TRY(b->d_kept.alloc(ctx, 1));
+  SB_TRY(b->d_leafval.alloc_zero(ctx, KN));
+  SB_TRY(b->d_fill.alloc_zero(ctx, KN));
+  SB_TRY(b->d_lvl.alloc_zero(ctx, 6 * K));
+  SB_TRY(b->d_rows0.alloc_zero(ctx, (size_t)K * b->n));
+  SB_TRY(b->d_rows1.alloc_zero(ctx, (size_t)K * b->n));
+  SB_TRY(b->d_kept.alloc_zero(ctx, 1));
   SB_CUDA(cudaMemsetAsync(b->d_kept.p, 0, 4, st));
-  SB_TRY(b->d_margin.alloc(ctx, b->n * K));
-  SB_TRY(b->d_delta.alloc(ctx, b->n * K));
-  SB_TRY(b->d_gpair.alloc(ctx, (size_t)K * b->n));
+  SB_TRY(b->d_margin.alloc_zero(ctx, b->n * K));
+  SB_TRY(b->d_delta.alloc_zero(ctx, b->n * K));
+  SB_TRY(b->d_gpair.alloc_zero(ctx, (size_t)K * b->n));
   const bool fixed = p->hist_precision == SB_HIST_FIXED;
-  if (fixed) SB_TRY(b->d_gpk.alloc(ctx, (size_t)K * b->n));
-  SB_TRY(b->d_maxabs.alloc(ctx, 2 * K));
+  if (fixed) SB_TRY(b->d_gpk.alloc_zero(ctx, (size_t)K * b->n));
+  SB_TRY(b->d_maxabs.alloc_zero(ctx, 2 * K));
   SB_CUDA(cudaMemsetAsync(b->d_maxabs.p, 0, 8 * K, st));
-  SB_TRY(b->d_shifts.alloc(ctx, 2 * K));
+  SB_TRY(b->d_shifts.alloc_zero(ctx, 2 * K));
   SB_CUDA(cudaMemsetAsync(b->d_shifts.p, 0, 8 * K, st));
-  SB_TRY(b->d_inv_scale.alloc(ctx, 2 * K));
-  SB_TRY(b->d_qerr.alloc(ctx, 1));
+  SB_TRY(b->d_inv_scale.alloc_zero(ctx, 2 * K));
+  SB_TRY(b->d_qerr.alloc_zero(ctx, 1));
   SB_CUDA(cudaMemsetAsync(b->d_qerr.p, 0, 8, st));
   if (b->lossguide) {  // every node keeps its histogram until its children are evaluated
-    SB_TRY(b->d_nhist.alloc(ctx, KN * HB * 16));
-    SB_TRY(b->d_heap.alloc(ctx, KN));
-    SB_TRY(b->d_heap_size.alloc(ctx, 2 * K));
-    SB_TRY(b->d_ndepth.alloc(ctx, KN));
+    SB_TRY(b->d_nhist.alloc_zero(ctx, KN * HB * 16));
+    SB_TRY(b->d_heap.alloc_zero(ctx, KN));
+    SB_TRY(b->d_heap_size.alloc_zero(ctx, 2 * K));
+    SB_TRY(b->d_ndepth.alloc_zero(ctx, KN));
   } else {
     const size_t hist_bytes = (size_t)K * b->maxw * HB * 16;
-    SB_TRY(b->d_hist0.alloc(ctx, hist_bytes));
-    SB_TRY(b->d_hist1.alloc(ctx, hist_bytes));
+    SB_TRY(b->d_hist0.alloc_zero(ctx, hist_bytes));
+    SB_TRY(b->d_hist1.alloc_zero(ctx, hist_bytes));
   }
-  SB_TRY(b->d_root_total.alloc(ctx, K));
-  SB_TRY(b->d_items.alloc(ctx, (size_t)K * b->maxw + K));
-  SB_TRY(b->d_prefix.alloc(ctx, (size_t)K * b->maxw + K + 1));
-  SB_TRY(b->d_item_count.alloc(ctx, 1));
+  SB_TRY(b->d_root_total.alloc_zero(ctx, K));
+  SB_TRY(b->d_items.alloc_zero(ctx, (size_t)K * b->maxw + K));
+  SB_TRY(b->d_prefix.alloc_zero(ctx, (size_t)K * b->maxw + K + 1));
+  SB_TRY(b->d_item_count.alloc_zero(ctx, 1));
   const int ptile_cap = (int)((size_t)K * ((b->n + PART_TILE - 1) / PART_TILE + b->maxn + 1));
-  SB_TRY(b->d_ptiles.alloc(ctx, ptile_cap));
-  SB_TRY(b->d_ptile_count.alloc(ctx, 1));
-  SB_TRY(b->d_pool.alloc(ctx, (size_t)K * F));
-  SB_TRY(b->d_pool_len.alloc(ctx, K));
-  SB_TRY(b->d_upool.alloc(ctx, (size_t)K * F));
-  SB_TRY(b->d_upool_len.alloc(ctx, K));
-  SB_TRY(b->d_pool_mask.alloc(ctx, (size_t)K * FW));
-  SB_TRY(b->d_mbuf.alloc(ctx, (size_t)K * b->maxw * F));
-  SB_TRY(b->d_frec.alloc(ctx, (size_t)K * b->maxw * F));
+  SB_TRY(b->d_ptiles.alloc_zero(ctx, ptile_cap));
+  SB_TRY(b->d_ptile_count.alloc_zero(ctx, 1));
+  SB_TRY(b->d_pool.alloc_zero(ctx, (size_t)K * F));
+  SB_TRY(b->d_pool_len.alloc_zero(ctx, K));
+  SB_TRY(b->d_upool.alloc_zero(ctx, (size_t)K * F));
+  SB_TRY(b->d_upool_len.alloc_zero(ctx, K));
+  SB_TRY(b->d_pool_mask.alloc_zero(ctx, (size_t)K * FW));
+  SB_TRY(b->d_mbuf.alloc_zero(ctx, (size_t)K * b->maxw * F));
+  SB_TRY(b->d_frec.alloc_zero(ctx, (size_t)K * b->maxw * F));
   {
     std::vector<uint32_t> usable(FW, 0u);
     for (int f = 0; f < F; ++f)
       if (g->h_foff[f + 1] - g->h_foff[f] >= 2) usable[f >> 5] |= 1u << (f & 31);
-    SB_TRY(b->d_usable.alloc(ctx, FW));
+    SB_TRY(b->d_usable.alloc_zero(ctx, FW));
     SB_CUDA(cudaMemcpyAsync(b->d_usable.p, usable.data(), FW * 4, cudaMemcpyHostToDevice, st));
   }
-  if (p->colsample_bylevel < 1.0 || p->colsample_bynode < 1.0) SB_TRY(b->d_samp.alloc(ctx, (size_t)1024 * F));
-  SB_TRY(b->d_tiles.alloc(ctx, g->tiles.size()));
+  if (p->colsample_bylevel < 1.0 || p->colsample_bynode < 1.0) SB_TRY(b->d_samp.alloc_zero(ctx, (size_t)1024 * F));
+  SB_TRY(b->d_tiles.alloc_zero(ctx, g->tiles.size()));
   SB_CUDA(cudaMemcpyAsync(b->d_tiles.p, g->tiles.data(), g->tiles.size() * sizeof(FeatureTile),
                           cudaMemcpyHostToDevice, st));
 
@@ -1942,7 +1942,7 @@ int booster_round_body(sb_booster* b, int apply_delta) {
   cudaEvent_t r0 = nullptr, r1 = nullptr;
   if (b->timing) {
     if (!b->d_hist_rows.p) {
-      SB_TRY(b->d_hist_rows.alloc(ctx, 1));
+      SB_TRY(b->d_hist_rows.alloc_zero(ctx, 1));
       SB_CUDA(cudaMemsetAsync(b->d_hist_rows.p, 0, 8, ctx->stream));
     }
     SB_CUDA(cudaEventCreate(&r0));

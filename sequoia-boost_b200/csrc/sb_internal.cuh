@@ -87,6 +87,14 @@ struct DBuf {
     if (count == 0) return SB_OK;
     return dalloc(c, (void**)&p, count * sizeof(T));
   }
+  // alloc, then zero on the context stream (state that is read before every
+  // path has written it then starts from zeros, not from the pool's leftovers)
+  int alloc_zero(sb_ctx* c, size_t count) {
+    int s = alloc(c, count);
+    if (s != SB_OK || count == 0) return s;
+    cudaError_t e = cudaMemsetAsync(p, 0, count * sizeof(T), c->stream);
+    return e == cudaSuccess ? SB_OK : cuda_status(e, "cudaMemsetAsync", __FILE__, __LINE__);
+  }
   void release() {
     if (p && ctx) dfree(ctx, p);
     p = nullptr;
