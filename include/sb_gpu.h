@@ -284,6 +284,29 @@ int sb_train(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
              const float* weights, const float* base_margin, const sb_train_params* p,
              int num_boost_round, sb_model** out);
 
+/* One job of sb_train_many: the arguments of sb_train, plus its outputs. */
+typedef struct sb_job {
+  const float* X;               /* [n_rows][n_cols], host */
+  size_t n_rows, n_cols;
+  const uint8_t* feature_types; /* or NULL */
+  float missing;
+  const float* labels;
+  const float* weights;         /* or NULL */
+  const float* base_margin;     /* or NULL */
+  const sb_train_params* params;
+  int32_t num_boost_round;
+  int32_t status;               /* out: SB_OK or the job's error */
+  sb_model* out;                /* out: the trained model (destroy with sb_model_destroy) */
+} sb_job;
+
+/* No counterpart in the reference (it trains one job per call; cv() runs its
+ * folds one after another). Trains independent jobs of any sizes together:
+ * each gets its own binned matrix and device booster, jobs are spread over
+ * n_streams streams (1..64), and round r of every job is issued before round
+ * r + 1 of any, so the GPU runs many jobs at once. Each model equals the one
+ * sb_train would give for its job. Returns the first failing job's status. */
+int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams);
+
 /* ------------------------------------------------------ model / predict */
 /* Uploads a host ensemble (BoostedModel) to the device. */
 int sb_model_create(sb_ctx* ctx, const sb_model_view* view, sb_model** out);

@@ -27,10 +27,11 @@ from .api import (  # noqa: F401
     TrainingParams,
     default_context,
     train,
+    train_many,
 )
 from ._abi import SbError  # noqa: F401
 
 __all__ = [
     "BoostedModel", "Booster", "Context", "DMatrix", "GHistIndex", "GpuBackend",
-    "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "train",
+    "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "train", "train_many",
 ]

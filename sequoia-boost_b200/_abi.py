@@ -126,6 +126,24 @@ class SbServerStats(ctypes.Structure):
         "mem_bytes", "mem_peak")]
 
 
+
+class SbJob(ctypes.Structure):
+    _fields_ = [
+        ("X", ctypes.POINTER(ctypes.c_float)),
+        ("n_rows", ctypes.c_size_t),
+        ("n_cols", ctypes.c_size_t),
+        ("feature_types", ctypes.POINTER(ctypes.c_uint8)),
+        ("missing", ctypes.c_float),
+        ("labels", ctypes.POINTER(ctypes.c_float)),
+        ("weights", ctypes.POINTER(ctypes.c_float)),
+        ("base_margin", ctypes.POINTER(ctypes.c_float)),
+        ("params", ctypes.POINTER(SbTrainParams)),
+        ("num_boost_round", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("out", ctypes.c_void_p),
+    ]
+
+
 SB_REQ_MARGIN = 0
 SB_REQ_CONTRIBS = 1
 
@@ -174,6 +192,7 @@ SIGNATURES = {
     "sb_booster_set_timing": (I32, [P, I32]),
     "sb_booster_stats_get": (I32, [P, ctypes.POINTER(SbBoosterStats)]),
     "sb_booster_stats_reset": (I32, [P]),
+    "sb_train_many": (I32, [P, ctypes.POINTER(SbJob), SZ, I32]),
     "sb_train": (I32, [P, F32P, SZ, SZ, U8P, ctypes.c_float, F32P, F32P, F32P,
                        ctypes.POINTER(SbTrainParams), I32, ctypes.POINTER(P)]),
     "sb_model_create": (I32, [P, ctypes.POINTER(SbModelView), ctypes.POINTER(P)]),

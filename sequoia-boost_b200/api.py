@@ -490,6 +490,43 @@ def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Co
     return BoostedModel(h, ctx)
 
 
+def train_many(jobs, n_streams=16, ctx: Context = None):
+    """Trains independent jobs together on the GPU (sb_train_many): `jobs` is
+    a list of (TrainingParams, DMatrix with labels, num_boost_round). Returns
+    one BoostedModel per job, each equal to what `train` gives for that job."""
+    ctx = ctx or default_context()
+    arr = (A.SbJob * len(jobs))()
+    keep = []
+    for i, (params, d, rounds) in enumerate(jobs):
+        if d.labels is None:
+            raise A.SbError(A.SB_ERR_INVALID_ARG, f"empty dataset: job {i} has no labels")
+        p, kp = params.to_c()
+        ft = d._ftypes()
+        bm = None
+        k = params.num_class if params.objective.startswith("multi:") else 1
+        if d.base_margin is not None:
+            bm = d.base_margin
+            if bm.size == d.n_rows and k > 1:
+                bm = np.repeat(bm.reshape(-1, 1), k, axis=1)
+            bm = np.ascontiguousarray(bm.reshape(-1), np.float32)
+        keep.append((p, kp, ft, bm, d))
+        j = arr[i]
+        j.X = A.ptr(d.data, ctypes.c_float)
+        j.n_rows, j.n_cols = d.n_rows, d.n_cols
+        j.feature_types = A.ptr(ft, ctypes.c_uint8)
+        j.missing = d.missing
+        j.labels = A.ptr(d.labels, ctypes.c_float)
+        j.weights = A.ptr(d.weights, ctypes.c_float)
+        j.base_margin = A.ptr(bm, ctypes.c_float)
+        j.params = ctypes.pointer(p)
+        j.num_boost_round = rounds
+    st = A.lib().sb_train_many(ctx.h, arr, len(jobs), n_streams)
+    models = [BoostedModel(ctypes.c_void_p(arr[i].out), ctx) if arr[i].out else None for i in range(len(jobs))]
+    del keep
+    A.check(st)
+    return models
+
+
 class HistTreeBuilder:
     """HistTreeBuilder::build (tree/builder/hist.rs:139-202) on the device."""
 

@@ -2,6 +2,9 @@
 #include <cstdarg>
 #include <cstring>
 
+#include <map>
+#include <mutex>
+
 #include "sb_internal.cuh"
 
 namespace sb {
@@ -34,6 +37,19 @@ int dalloc(sb_ctx* ctx, void** p, size_t bytes) {
     set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return SB_ERR_OOM;
   }
+  return SB_OK;
+}
+
+int raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> set;
+  int dev = 0;
+  SB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = set[std::make_pair(func, dev)];
+  if (bytes <= cur) return SB_OK;
+  SB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
   return SB_OK;
 }
 

@@ -2112,14 +2112,14 @@ int booster_collect_timing(sb_booster* b) {
 
 int booster_set_eval_smem(sb_booster* b) {
   int esm = (int)eval_smem(b);
-  SB_CUDA(cudaFuncSetAttribute(k_eval_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
-  SB_CUDA(cudaFuncSetAttribute(k_eval_pick, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
-  SB_CUDA(cudaFuncSetAttribute(k_eval_records, cudaFuncAttributeMaxDynamicSharedMemorySize, esm));
+  SB_TRY(raise_smem_limit((const void*)k_eval_scan, (size_t)esm));
+  SB_TRY(raise_smem_limit((const void*)k_eval_pick, (size_t)esm));
+  SB_TRY(raise_smem_limit((const void*)k_eval_records, (size_t)esm));
   if (b->lossguide) {
     const size_t heap_smem = (size_t)b->maxn * sizeof(HeapEnt);
     SB_REQUIRE(heap_smem <= b->ctx->smem_optin, SB_ERR_UNSUPPORTED, "lossguide queue of %d nodes exceeds shared memory",
                b->maxn);
-    SB_CUDA(cudaFuncSetAttribute(k_lg_heap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heap_smem));
+    SB_TRY(raise_smem_limit((const void*)k_lg_heap, (size_t)heap_smem));
   }
   return SB_OK;
 }

@@ -292,8 +292,8 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
       g->h_fmiss[f] = t.nbins + (f - t.f0);
     }
   g->hist_smem_bytes = maxb;
-  SB_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));
-  SB_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxb));
+  SB_TRY(raise_smem_limit((const void*)k_hist<false>, (size_t)maxb));
+  SB_TRY(raise_smem_limit((const void*)k_hist<true>, (size_t)maxb));
   return SB_OK;
 }
 

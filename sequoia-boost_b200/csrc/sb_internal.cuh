@@ -69,6 +69,10 @@ namespace sb {
 
 // Stream-ordered device allocation (pool-backed, cached across calls).
 int dalloc(sb_ctx* ctx, void** p, size_t bytes);
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`; never lowers it (another index, booster or model of the
+// process may launch the same kernel with more).
+int raise_smem_limit(const void* func, size_t bytes);
 void dfree(sb_ctx* ctx, void* p);
 
 template <typename T>

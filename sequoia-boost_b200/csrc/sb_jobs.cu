@@ -1,0 +1,72 @@
+// sb_jobs.cu — sb_train_many: many independent training jobs (k-fold splits,
+// parameter sweeps) of uneven sizes trained together on one GPU.
+//
+// Each job gets its own binned matrix and device booster (train(), learner/
+// train.rs:107-113, per job). Jobs are spread round-robin over a pool of
+// streams; the host then issues round r of every unfinished job before
+// round r + 1 of any, so the GPU always holds work of many jobs at once and
+// small jobs fill the SMs that one small job alone would leave idle. From its
+// third round on, a job's round is one CUDA-graph launch, so issuing a round
+// of every job costs the host a few microseconds per job.
+#include <algorithm>
+#include <vector>
+
+#include "sb_internal.cuh"
+
+extern "C" {
+
+int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams) {
+  using namespace sb;
+  SB_REQUIRE(ctx && (jobs || n_jobs == 0), SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(n_streams >= 1 && n_streams <= 64, SB_ERR_INVALID_ARG, "n_streams must be in [1, 64]");
+  for (size_t j = 0; j < n_jobs; ++j) {
+    jobs[j].out = nullptr;
+    jobs[j].status = SB_OK;
+    SB_REQUIRE(jobs[j].X && jobs[j].labels && jobs[j].params, SB_ERR_INVALID_ARG, "job %zu: NULL argument", j);
+    SB_REQUIRE(jobs[j].num_boost_round >= 0, SB_ERR_INVALID_ARG, "job %zu: negative num_boost_round", j);
+  }
+  SB_CUDA(cudaSetDevice(ctx->device));
+  const int S = (int)std::min<size_t>((size_t)n_streams, std::max<size_t>(n_jobs, 1));
+  std::vector<sb_ctx*> sctx(S, nullptr);
+  std::vector<sb_ghist*> gh(n_jobs, nullptr);
+  std::vector<sb_booster*> bo(n_jobs, nullptr);
+  int rc = SB_OK;
+  for (int s = 0; s < S && rc == SB_OK; ++s) rc = sb_ctx_create(ctx->device, &sctx[s]);
+  // set-up: bin each job's matrix and create its booster on its stream
+  for (size_t j = 0; j < n_jobs && rc == SB_OK; ++j) {
+    sb_job& jb = jobs[j];
+    sb_ctx* c = sctx[j % S];
+    int s = sb_train_params_validate(jb.params);
+    if (s == SB_OK)
+      s = sb_ghist_create(c, jb.X, jb.n_rows, jb.n_cols, jb.feature_types, jb.missing, jb.params->max_bin, &gh[j]);
+    if (s == SB_OK) s = sb_booster_create(c, gh[j], jb.params, jb.labels, jb.weights, jb.base_margin, &bo[j]);
+    jb.status = s;
+  }
+  // rounds, interleaved across jobs
+  int max_rounds = 0;
+  for (size_t j = 0; j < n_jobs; ++j) max_rounds = std::max(max_rounds, jobs[j].num_boost_round);
+  for (int r = 0; r < max_rounds && rc == SB_OK; ++r)
+    for (size_t j = 0; j < n_jobs; ++j)
+      if (jobs[j].status == SB_OK && r < jobs[j].num_boost_round) jobs[j].status = sb_booster_update(bo[j], 1);
+  // models
+  for (size_t j = 0; j < n_jobs && rc == SB_OK; ++j)
+    if (jobs[j].status == SB_OK) {
+      jobs[j].status = sb_booster_model(bo[j], &jobs[j].out);
+      if (jobs[j].out) jobs[j].out->ctx = ctx;  // the job streams end here; the model lives on
+    }
+  for (size_t j = 0; j < n_jobs; ++j) {
+    sb_booster_destroy(bo[j]);
+    sb_ghist_destroy(gh[j]);
+  }
+  for (sb_ctx* c : sctx)
+    if (c) sb_ctx_destroy(c);
+  if (rc != SB_OK) return rc;
+  for (size_t j = 0; j < n_jobs; ++j)
+    if (jobs[j].status != SB_OK) {
+      set_error("job %zu failed with status %d", j, jobs[j].status);
+      return jobs[j].status;
+    }
+  return SB_OK;
+}
+
+}  // extern "C"

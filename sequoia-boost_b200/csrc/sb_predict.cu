@@ -459,9 +459,9 @@ int model_upload(sb_model* m) {
   D.n_shap_chunks = (int)chunks.size();
   {  // shared memory of the TreeSHAP blocks: f32 partials of SHAP_ROWS rows
     const int smem = (int)std::min<size_t>((size_t)m->n_features * SHAP_ROWS * 4, ctx->smem_optin);
-    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SB_CUDA(cudaFuncSetAttribute(k_shap_paths<SHAP_MAXD + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SB_TRY(raise_smem_limit((const void*)k_shap_paths<5>, (size_t)smem));
+    SB_TRY(raise_smem_limit((const void*)k_shap_paths<9>, (size_t)smem));
+    SB_TRY(raise_smem_limit((const void*)k_shap_paths<SHAP_MAXD + 1>, (size_t)smem));
   }
   D.max_path_len = maxlen;
   {
