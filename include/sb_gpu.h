@@ -342,16 +342,19 @@ int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_col
  * ensemble kept resident in HBM answers margin requests (the output of
  * sb_predict_margin with ntree_limit 0 and no base_margin, [n][K]) and
  * TreeSHAP requests (the output of sb_predict_contribs, [n][K][n_cols+1])
- * from any number of threads, with continuous batching: a dispatcher thread
- * joins runs of queued requests of one kind into device batches, admits a
- * batch when its buffers fit in the free part of the loop's memory budget,
- * and keeps up to n_slots margin batches (high stream priority) and
- * max(1, n_slots / 2) TreeSHAP batches (low priority) in flight, each on its
- * own stream. Host buffers may be pageable; page-locked X and out make the
- * copies asynchronous. Set CUDA_DEVICE_MAX_CONNECTIONS to at least
- * 1.5 * n_slots + 2 (e.g. 32) in the environment before the process's first
- * CUDA call: with the default 8 hardware work queues, streams share queues and
- * a margin batch can wait behind a TreeSHAP kernel of another stream. */
+ * from any number of threads, with continuous batching: requests queue in
+ * three lanes (margin requests of at most 4096 rows, larger margin requests,
+ * TreeSHAP requests); a dispatcher thread joins runs of queued requests of one
+ * lane into device batches, admits a batch when its buffers fit in the free
+ * part of the loop's memory budget, and keeps up to max(1, n_slots / 2) small
+ * margin batches (highest stream priority), max(1, n_slots - n_slots / 2)
+ * larger margin batches (middle priority) and max(1, n_slots / 2) TreeSHAP
+ * batches (lowest priority) in flight, each on its own stream. Host buffers
+ * may be pageable; page-locked X and out make the copies asynchronous. Set
+ * CUDA_DEVICE_MAX_CONNECTIONS to at least 1.5 * n_slots + 2 (e.g. 32) in the
+ * environment before the process's first CUDA call: with the default 8
+ * hardware work queues, streams share queues and a margin batch can wait
+ * behind a TreeSHAP kernel of another stream. */
 typedef struct sb_server sb_server;
 enum { SB_REQ_MARGIN = 0, SB_REQ_CONTRIBS = 1 };
 typedef struct sb_server_stats {
@@ -362,8 +365,8 @@ typedef struct sb_server_stats {
   uint64_t mem_bytes, mem_peak;  /* budget and the most of it in use */
 } sb_server_stats;
 /* mem_bytes: device memory for request buffers (0 = half of what is free
- * now); n_slots: margin batches in flight (1..64). The model must outlive
- * the loop. */
+ * now); n_slots: margin batches in flight over both margin lanes (1..64). The
+ * model must outlive the loop. */
 int sb_server_create(sb_ctx* ctx, sb_model* m, size_t mem_bytes, int n_slots, sb_server** out);
 /* Queues a request; X [n_rows][n_cols] and out stay owned by the caller and
  * must stay valid until sb_server_wait returns for the ticket. */

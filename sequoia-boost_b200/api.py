@@ -152,9 +152,9 @@ class Context:
     def launch_count(self):
         return A.lib().sb_ctx_launch_count(self.h)
 
-    def __del__(self):
+    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
         if getattr(self, "h", None):
-            A.lib().sb_ctx_destroy(self.h)
+            _A.lib().sb_ctx_destroy(self.h)
             self.h = None
 
 
@@ -289,9 +289,9 @@ class GHistIndex:
         g[lb == 0xFFFF] = 0xFFFFFFFF
         return g
 
-    def __del__(self):
+    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
         if getattr(self, "h", None):
-            A.lib().sb_ghist_destroy(self.h)
+            _A.lib().sb_ghist_destroy(self.h)
             self.h = None
 
 
@@ -459,9 +459,9 @@ class BoostedModel:
                                             d.missing, A.ptr(out, ctypes.c_float)))
         return out.reshape(-1)
 
-    def __del__(self):
+    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
         if getattr(self, "h", None):
-            A.lib().sb_model_destroy(self.h)
+            _A.lib().sb_model_destroy(self.h)
             self.h = None
 
 
@@ -610,9 +610,9 @@ class Booster:
     def reset_stats(self):
         A.check(A.lib().sb_booster_stats_reset(self.h))
 
-    def __del__(self):
+    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
         if getattr(self, "h", None):
-            A.lib().sb_booster_destroy(self.h)
+            _A.lib().sb_booster_destroy(self.h)
             self.h = None
 
 
@@ -666,5 +666,7 @@ class Server:
             self.h = None
             self._pending.clear()
 
-    def __del__(self):
-        self.close()
+    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
+        if getattr(self, "h", None):
+            _A.lib().sb_server_destroy(self.h)
+            self.h = None

@@ -3,20 +3,25 @@
 // (predict_contribs, learner/shap.rs:321-367) requests with continuous
 // batching.
 //
-//   submit  : any thread; the request joins its kind's FIFO queue.
-//   dispatcher thread : each kind has its own slots (a slot is a CUDA
-//             stream: high priority for margins, low for TreeSHAP). Whenever
-//             a slot is free, the dispatcher takes the longest run at the
-//             head of that kind's queue sharing a missing-value marker, up to
-//             a row cap, and admits it if its device buffers fit in the free
-//             part of the loop's memory budget (first-fit arena); otherwise
-//             that queue's head waits until a finishing batch frees memory.
-//             The batch's rows are copied into one device buffer, run as one
-//             set of kernel launches and copied back per request. Several
-//             batches are in flight at once, so requests that arrive while
-//             others are on the GPU are admitted as slots and memory free up;
-//             heavy TreeSHAP work never takes a margin slot, and its short
-//             kernel blocks give margin kernels SMs as soon as they arrive.
+//   submit  : any thread; the request joins one of three FIFO lanes: small
+//             margin requests (at most SMALL_ROWS rows), larger margin
+//             requests, TreeSHAP requests.
+//   dispatcher thread : each lane has its own slots (a slot is a CUDA
+//             stream; small margins get the highest stream priority, larger
+//             margins the middle one, TreeSHAP the lowest). Whenever a slot
+//             is free, the dispatcher takes the longest run at the head of
+//             that lane's queue sharing a missing-value marker, up to the
+//             lane's row cap, and admits it if its device buffers fit in the
+//             free part of the loop's memory budget (first-fit arena);
+//             otherwise that lane's head waits until a finishing batch frees
+//             memory. The batch's rows are copied into one device buffer,
+//             run as one set of kernel launches and copied back per request.
+//             Several batches are in flight at once, so requests that arrive
+//             while others are on the GPU are admitted as slots and memory
+//             free up. A small request never queues behind a large batch, and
+//             since every kernel is made of short blocks, the block scheduler
+//             hands the SMs to the higher-priority stream as soon as its
+//             kernel arrives.
 //   completion : a host function queued behind each batch flags the slot; the
 //             dispatcher then marks the requests done and frees their memory.
 //
@@ -48,8 +53,15 @@ struct Server;
 namespace {
 
 constexpr size_t ALIGN = 256;
-constexpr size_t MARGIN_BATCH_ROWS = 65536;    // row cap of one margin batch
-constexpr size_t CONTRIBS_BATCH_ROWS = 65536;  // row cap of one TreeSHAP batch
+constexpr size_t SMALL_ROWS = 4096;  // margin requests up to this size take the small lane
+enum { LANE_SMALL = 0, LANE_MARGIN = 1, LANE_CONTRIBS = 2, N_LANES = 3 };
+constexpr size_t LANE_BATCH_ROWS[N_LANES] = {16384, 65536, 65536};  // row cap of one batch
+
+int lane_kind(int lane) { return lane == LANE_CONTRIBS ? SB_REQ_CONTRIBS : SB_REQ_MARGIN; }
+int lane_of(int kind, size_t rows) {
+  if (kind == SB_REQ_CONTRIBS) return LANE_CONTRIBS;
+  return rows <= SMALL_ROWS ? LANE_SMALL : LANE_MARGIN;
+}
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -117,7 +129,7 @@ struct Arena {
 struct Slot {
   Server* srv = nullptr;
   cudaStream_t st = nullptr;
-  int kind = 0;
+  int lane = 0;
   bool busy = false;
   bool finished = false;  // set by the completion host function (under the mutex)
   std::vector<std::shared_ptr<Request>> reqs;
@@ -139,11 +151,11 @@ struct Server {
   std::mutex mu;
   std::condition_variable cv;       // dispatcher wake-ups
   std::condition_variable done_cv;  // request completions
-  std::deque<std::shared_ptr<Request>> queue[2];  // per kind
+  std::deque<std::shared_ptr<Request>> queue[N_LANES];
   std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
   uint64_t next_ticket = 1;
   bool stop = false;
-  bool mem_blocked[2] = {false, false};  // a queue head waits for memory to be freed
+  bool mem_blocked[N_LANES] = {};  // a lane's head waits for memory to be freed
   std::thread worker;
   sb_server_stats stats{};
 
@@ -206,17 +218,18 @@ struct Server {
     s->busy = false;
     s->finished = false;
     arena.release(s->mem_off, s->mem_bytes);
-    mem_blocked[0] = mem_blocked[1] = false;
+    for (bool& b : mem_blocked) b = false;
     done_cv.notify_all();
   }
 
-  // Takes the longest admissible run at the head of the queue into slot s.
-  // Returns the run's rows, 0 when the head must wait for memory.
-  size_t admit(Slot* s, int kind, float* miss_out) {
-    std::deque<std::shared_ptr<Request>>& queue = this->queue[kind];
+  // Takes the longest admissible run at the head of a lane's queue into slot
+  // s. Returns the run's rows, 0 when the head must wait for memory.
+  size_t admit(Slot* s, int lane, float* miss_out) {
+    std::deque<std::shared_ptr<Request>>& queue = this->queue[lane];
+    const int kind = lane_kind(lane);
     const float miss = queue.front()->missing;
     const bool miss_nan = std::isnan(miss);
-    const size_t cap = kind == SB_REQ_MARGIN ? MARGIN_BATCH_ROWS : CONTRIBS_BATCH_ROWS;
+    const size_t cap = LANE_BATCH_ROWS[lane];
     size_t rows = 0, take = 0;
     for (auto& r : queue) {
       const bool same_miss = miss_nan ? std::isnan(r->missing) : r->missing == miss;
@@ -247,14 +260,24 @@ struct Server {
     return rows;
   }
 
-  Slot* free_slot(int kind) {
+  Slot* free_slot(int lane) {
     for (auto& s : slots)
-      if (s->kind == kind && !s->busy) return s.get();
+      if (s->lane == lane && !s->busy) return s.get();
     return nullptr;
   }
 
-  bool can_admit(int kind) {
-    return !queue[kind].empty() && !mem_blocked[kind] && free_slot(kind) != nullptr;
+  bool can_admit(int lane) {
+    return !queue[lane].empty() && !mem_blocked[lane] && free_slot(lane) != nullptr;
+  }
+  bool any_admissible() {
+    for (int l = 0; l < N_LANES; ++l)
+      if (can_admit(l)) return true;
+    return false;
+  }
+  bool queues_empty() const {
+    for (int l = 0; l < N_LANES; ++l)
+      if (!queue[l].empty()) return false;
+    return true;
   }
 
   void run() {
@@ -263,10 +286,11 @@ struct Server {
     for (;;) {
       for (auto& s : slots)
         if (s->busy && s->finished) finish(s.get());
-      for (int kind = 0; kind < 2; ++kind) {
-        std::deque<std::shared_ptr<Request>>& queue = this->queue[kind];
-        while (can_admit(kind)) {
-          Slot* slot = free_slot(kind);
+      for (int lane = 0; lane < N_LANES; ++lane) {  // highest priority first
+        std::deque<std::shared_ptr<Request>>& queue = this->queue[lane];
+        const int kind = lane_kind(lane);
+        while (can_admit(lane)) {
+          Slot* slot = free_slot(lane);
           if (batch_bytes(kind, queue.front()->n) > arena.size) {  // can never fit
             auto r = queue.front();
             queue.pop_front();
@@ -279,9 +303,9 @@ struct Server {
             continue;
           }
           float miss = NAN;
-          const size_t rows = admit(slot, kind, &miss);
+          const size_t rows = admit(slot, lane, &miss);
           if (rows == 0) {  // the head waits until a finishing batch frees memory
-            mem_blocked[kind] = true;
+            mem_blocked[lane] = true;
             stats.memory_waits++;
             break;
           }
@@ -295,7 +319,7 @@ struct Server {
       }
       bool any_busy = false;
       for (auto& s : slots) any_busy = any_busy || s->busy;
-      if (stop && queue[0].empty() && queue[1].empty() && !any_busy) break;
+      if (stop && queues_empty() && !any_busy) break;
       // sleep (releasing the mutex, which the completion host functions
       // need) until a batch finishes, a queued request can be admitted, or
       // the loop may stop
@@ -305,8 +329,8 @@ struct Server {
           if (s->busy && s->finished) return true;
           busy = busy || s->busy;
         }
-        if (can_admit(0) || can_admit(1)) return true;
-        return stop && queue[0].empty() && queue[1].empty() && !busy;
+        if (any_admissible()) return true;
+        return stop && queues_empty() && !busy;
       });
     }
   }
@@ -355,17 +379,19 @@ int sb_server_create(sb_ctx* ctx, sb_model* m, size_t mem_bytes, int n_slots, sb
     return SB_ERR_OOM;
   }
   s->arena.init(s->d_mem, mem_bytes);
-  int lo_prio = 0, hi_prio = 0;
+  int lo_prio = 0, hi_prio = 0;  // numerically lower is higher priority
   SB_CUDA(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
-  const int n_shap = std::max(1, n_slots / 2);
-  for (int i = 0; i < n_slots + n_shap; ++i) {  // margin slots, then TreeSHAP slots
-    std::unique_ptr<Slot> sl(new Slot);
-    sl->srv = s.get();
-    sl->kind = i < n_slots ? SB_REQ_MARGIN : SB_REQ_CONTRIBS;
-    SB_CUDA(cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking,
-                                         sl->kind == SB_REQ_MARGIN ? hi_prio : lo_prio));
-    s->slots.push_back(std::move(sl));
-  }
+  const int lane_slots[N_LANES] = {std::max(1, n_slots / 2), std::max(1, n_slots - n_slots / 2),
+                                   std::max(1, n_slots / 2)};
+  const int lane_prio[N_LANES] = {hi_prio, (lo_prio + hi_prio) / 2, lo_prio};
+  for (int lane = 0; lane < N_LANES; ++lane)
+    for (int i = 0; i < lane_slots[lane]; ++i) {
+      std::unique_ptr<Slot> sl(new Slot);
+      sl->srv = s.get();
+      sl->lane = lane;
+      SB_CUDA(cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, lane_prio[lane]));
+      s->slots.push_back(std::move(sl));
+    }
   s->stats.mem_bytes = mem_bytes;
   s->worker = std::thread([p = s.get()] { p->run(); });
   *out = s.release();
@@ -397,7 +423,7 @@ int sb_server_submit(sb_server* s, int kind, const float* X, size_t n_rows, size
       r->t_done = r->t_submit;
       s->stats.completed++;
     } else {
-      s->queue[kind].push_back(r);
+      s->queue[lane_of(kind, n_rows)].push_back(r);
     }
     *ticket = r->ticket;
   }

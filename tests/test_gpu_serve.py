@@ -67,6 +67,33 @@ def test_results_alone_equal_results_in_the_mix(sb, served):
         srv.close()
 
 
+def test_small_and_large_margin_lanes(sb, served):
+    """Margin requests on both sides of the small-lane bound (4096 rows) and
+    TreeSHAP requests, submitted together, each get their own rows' results."""
+    m, x = served
+    rng = np.random.default_rng(5)
+    sizes = [1, 4096, 4097, 19000, 37, 4095, 12000, 2, 8000, 4096]
+    reqs = []
+    for i, n in enumerate(sizes):
+        idx = rng.integers(0, x.shape[0], n)
+        reqs.append(("contribs" if i % 5 == 4 else "margin", np.ascontiguousarray(x[idx])))
+    srv = sb.Server(m, mem_bytes=512 << 20, n_slots=2)
+    try:
+        tickets = [srv.submit(xr, kind=k) for k, xr in reqs]
+        for (kind, xr), t in zip(reqs, tickets):
+            got, _ = srv.wait(t, timeout_ms=60000)
+            d = sb.DMatrix(xr)
+            if kind == "margin":
+                assert np.array_equal(got, m.predict_margin(d)), len(xr)
+            else:
+                want = m.predict_contribs(d)
+                assert np.max(np.abs(got - want)) <= 1e-5 * max(1.0, np.max(np.abs(want)))
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["failed"] == 0
+    finally:
+        srv.close()
+
+
 def test_admission_waits_for_memory_and_rejects_what_never_fits(sb, served):
     m, x = served
     # a budget that holds a few 2000-row margin batches, not all of them
