@@ -336,6 +336,16 @@ int sb_predict(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float 
  * [n][K][n_cols+1], bias last. */
 int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
                         float missing, float* out);
+/* BoostedModel::predict_leaf, learner/model.rs:330-341: out [n][n_trees]
+ * leaf node ids (RegTree::leaf_id_with, regtree.rs:213-242). */
+int sb_predict_leaf(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float missing,
+                    uint32_t* out);
+/* BoostedModel::predict_interactions, learner/shap.rs:395-509: out
+ * [n][K][n_cols+1][n_cols+1]; [F][F] holds the sum of the trees' expected
+ * values (no base score), the rest of the last row and column is 0. On a
+ * B200: up to 239 features (an f32 matrix per row in shared memory). */
+int sb_predict_interactions(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
+                            float missing, float* out);
 
 /* -------------------------------------------------------- serving loop */
 /* No counterpart in the reference (it predicts one call at a time). A tree

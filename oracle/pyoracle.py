@@ -95,6 +95,9 @@ SIGS = {
                                           SZ, FP]),
     "orc_predict_contribs": (ctypes.c_int, [ctypes.POINTER(ModelView), FP, SZ, SZ, ctypes.c_float,
                                             FP]),
+    "orc_predict_leaf": (ctypes.c_int, [ctypes.POINTER(ModelView), FP, SZ, SZ, ctypes.c_float, U32P]),
+    "orc_predict_interactions": (ctypes.c_int, [ctypes.POINTER(ModelView), FP, SZ, SZ, ctypes.c_float,
+                                                FP]),
     "orc_gradient": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_double, FP, FP, FP, SZ,
                             ctypes.POINTER(GradPair)]),
     "orc_pred_transform": (None, [ctypes.c_int, ctypes.c_int, FP, SZ]),
@@ -299,6 +302,25 @@ class Oracle:
         out = np.zeros(x.shape[0] * k * (x.shape[1] + 1), np.float32)
         self.lib.orc_predict_contribs(ctypes.byref(v), _p(x, ctypes.c_float), x.shape[0], x.shape[1],
                                       missing, _p(out, ctypes.c_float))
+        return out
+
+    def predict_leaf(self, arrays, x, missing=float("nan")):
+        """[n][n_trees] leaf node ids (predict_leaf, model.rs:330-341)."""
+        x = np.ascontiguousarray(x, np.float32)
+        v, keep = self._view(arrays, 0.0, 0, x.shape[1])
+        out = np.zeros((x.shape[0], v.n_trees), np.uint32)
+        self.lib.orc_predict_leaf(ctypes.byref(v), _p(x, ctypes.c_float), x.shape[0], x.shape[1], missing,
+                                  _p(out, ctypes.c_uint32))
+        return out
+
+    def predict_interactions(self, arrays, x, base_score, num_class=0, missing=float("nan")):
+        """[n][K][F+1][F+1] flattened (predict_interactions, shap.rs:395-509)."""
+        x = np.ascontiguousarray(x, np.float32)
+        v, keep = self._view(arrays, base_score, num_class, x.shape[1])
+        k = num_class if num_class >= 2 else 1
+        out = np.zeros(x.shape[0] * k * (x.shape[1] + 1) ** 2, np.float32)
+        self.lib.orc_predict_interactions(ctypes.byref(v), _p(x, ctypes.c_float), x.shape[0], x.shape[1],
+                                          missing, _p(out, ctypes.c_float))
         return out
 
 

@@ -912,10 +912,14 @@ double unwound_path_sum(const std::vector<PathEl>& path, size_t pi) {  // shap.r
   }
   return total;
 }
-void tree_shap(const OTree& t, size_t nidx, std::vector<PathEl> path, double pz, double po,
-               int64_t pf, const float* row, float missing, double* phi) {
-  // tree_shap_cond with condition 0, shap.rs:165-283
-  extend_path(path, pz, po, pf);
+void tree_shap_cond(const OTree& t, size_t nidx, std::vector<PathEl> path, double pz, double po,
+                    int64_t pf, const float* row, float missing, double* phi, int cond, int64_t cf,
+                    double cfrac) {
+  // tree_shap_cond, shap.rs:165-283: cond 0 = ordinary TreeSHAP; +1 / -1 =
+  // feature cf fixed present / absent (kept off the path, its weight carried
+  // in cfrac)
+  if (cfrac == 0.0) return;
+  if (cond == 0 || cf != pf) extend_path(path, pz, po, pf);
   const sb_node& nd = t.nodes[nidx];
   size_t ud = path.size() - 1;
   if (nd.left == -1) {
@@ -923,7 +927,7 @@ void tree_shap(const OTree& t, size_t nidx, std::vector<PathEl> path, double pz,
     for (size_t i = 1; i <= ud; ++i) {
       double w = unwound_path_sum(path, i);
       const PathEl& el = path[i];
-      phi[el.feature] += w * (el.one - el.zero) * leaf * 1.0;
+      phi[el.feature] += w * (el.one - el.zero) * leaf * cfrac;
     }
     return;
   }
@@ -947,8 +951,18 @@ void tree_shap(const OTree& t, size_t nidx, std::vector<PathEl> path, double pz,
       break;
     }
   }
-  tree_shap(t, hot, path, hz * iz, io, si, row, missing, phi);
-  tree_shap(t, cold, std::move(path), cz * iz, 0.0, si, row, missing, phi);
+  double hot_cf = cfrac, cold_cf = cfrac;
+  if (cond > 0 && si == cf) cold_cf = 0.0;
+  else if (cond < 0 && si == cf) {
+    hot_cf *= hz;
+    cold_cf *= cz;
+  }
+  tree_shap_cond(t, hot, path, hz * iz, io, si, row, missing, phi, cond, cf, hot_cf);
+  tree_shap_cond(t, cold, std::move(path), cz * iz, 0.0, si, row, missing, phi, cond, cf, cold_cf);
+}
+void tree_shap(const OTree& t, size_t nidx, std::vector<PathEl> path, double pz, double po,
+               int64_t pf, const float* row, float missing, double* phi) {
+  tree_shap_cond(t, nidx, std::move(path), pz, po, pf, row, missing, phi, 0, -1, 1.0);
 }
 double node_mean_value(const OTree& t, size_t id) {  // shap.rs:288-302
   const sb_node& nd = t.nodes[id];
@@ -1347,6 +1361,58 @@ int orc_predict_contribs(const sb_model_view* v, const float* X, size_t n, size_
       acc[off + F] += means[t];
     }
     for (size_t i = 0; i < K * width; ++i) out[r * K * width + i] = (float)acc[i];
+  }
+  return 0;
+}
+
+int orc_predict_leaf(const sb_model_view* v, const float* X, size_t n, size_t F, float missing,
+                     uint32_t* out) {
+  // predict_leaf, learner/model.rs:330-341: [n][T] leaf node ids
+  std::vector<OTree> trees;
+  view_to_trees(v, trees);
+  const size_t T = trees.size();
+  for (size_t r = 0; r < n; ++r)
+    for (size_t t = 0; t < T; ++t) out[r * T + t] = (uint32_t)leaf_id(trees[t], X + r * F, missing);
+  return 0;
+}
+
+int orc_predict_interactions(const sb_model_view* v, const float* X, size_t n, size_t F, float missing,
+                             float* out) {
+  // predict_interactions, learner/shap.rs:395-509: [n][K][F+1][F+1]
+  std::vector<OTree> trees;
+  view_to_trees(v, trees);
+  const int K = v->num_class >= 2 ? v->num_class : 1;
+  const size_t width = F + 1, mw = width * width;
+  std::vector<double> means(trees.size());
+  for (size_t t = 0; t < trees.size(); ++t) means[t] = node_mean_value(trees[t], 0);
+  std::vector<double> diag(K * width), on(K * width), off(K * width), mat(K * mw);
+  for (size_t r = 0; r < n; ++r) {
+    const float* row = X + r * F;
+    std::fill(diag.begin(), diag.end(), 0.0);
+    std::fill(mat.begin(), mat.end(), 0.0);
+    for (size_t t = 0; t < trees.size(); ++t) {
+      const size_t base = (t % K) * width;
+      tree_shap_cond(trees[t], 0, {}, 1.0, 1.0, -1, row, missing, diag.data() + base, 0, -1, 1.0);
+      diag[base + F] += means[t];
+    }
+    for (int c = 0; c < K; ++c)
+      for (size_t j = 0; j < width; ++j) mat[c * mw + j * width + j] = diag[c * width + j];
+    for (size_t j = 0; j < F; ++j) {
+      std::fill(on.begin(), on.end(), 0.0);
+      std::fill(off.begin(), off.end(), 0.0);
+      for (size_t t = 0; t < trees.size(); ++t) {
+        const size_t base = (t % K) * width;
+        tree_shap_cond(trees[t], 0, {}, 1.0, 1.0, -1, row, missing, on.data() + base, 1, (int64_t)j, 1.0);
+        tree_shap_cond(trees[t], 0, {}, 1.0, 1.0, -1, row, missing, off.data() + base, -1, (int64_t)j, 1.0);
+      }
+      for (int c = 0; c < K; ++c)
+        for (size_t kk = 0; kk < width; ++kk) {
+          const double val = 0.5 * (on[c * width + kk] - off[c * width + kk]);
+          mat[c * mw + j * width + kk] += val;
+          mat[c * mw + j * width + j] -= val;
+        }
+    }
+    for (size_t i = 0; i < K * mw; ++i) out[r * K * mw + i] = (float)mat[i];
   }
   return 0;
 }

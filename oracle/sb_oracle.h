@@ -75,6 +75,12 @@ int orc_predict_margin(const sb_model_view* v, const float* X, size_t n, size_t 
                        float missing, const float* base_margin, size_t ntree_limit, float* out);
 int orc_predict_contribs(const sb_model_view* v, const float* X, size_t n, size_t F,
                          float missing, float* out);
+/* predict_leaf (learner/model.rs:330-341): out [n][n_trees] leaf node ids. */
+int orc_predict_leaf(const sb_model_view* v, const float* X, size_t n, size_t F, float missing,
+                     uint32_t* out);
+/* predict_interactions (learner/shap.rs:395-509): out [n][K][F+1][F+1]. */
+int orc_predict_interactions(const sb_model_view* v, const float* X, size_t n, size_t F,
+                             float missing, float* out);
 /* Objective::gradient over margins [n][K] -> out [n][K]. */
 void orc_gradient(int objective, int num_class, double scale_pos_weight, const float* preds,
                   const float* labels, const float* weights, size_t n, sb_gradpair* out);

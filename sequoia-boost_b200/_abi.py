@@ -203,6 +203,8 @@ SIGNATURES = {
     "sb_predict_margin": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, SZ, F32P]),
     "sb_predict": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P]),
     "sb_predict_contribs": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
+    "sb_predict_leaf": (I32, [P, F32P, SZ, SZ, ctypes.c_float, ctypes.POINTER(ctypes.c_uint32)]),
+    "sb_predict_interactions": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
     "sb_server_create": (I32, [P, P, SZ, I32, ctypes.POINTER(P)]),
     "sb_server_submit": (I32, [P, I32, F32P, SZ, SZ, ctypes.c_float, F32P, ctypes.POINTER(ctypes.c_uint64)]),
     "sb_server_wait": (I32, [P, ctypes.c_uint64, I32, ctypes.POINTER(ctypes.c_double)]),

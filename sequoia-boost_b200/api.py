@@ -1,6 +1,7 @@
 """Python mirror of the reference crate's API over libsb_gpu.so (see __init__)."""
 import ctypes
 import math
+import sys
 from dataclasses import dataclass, field
 from typing import List, Optional
 
@@ -134,7 +135,38 @@ class _ParamsBuilder:
         return self.params
 
 
-class Context:
+class _Native:
+    """Owner of a native handle `h`. Its destroy call waits until every object
+    created on it (a model on a context, a server on a model) has destroyed
+    its own handle: the finalizers of garbage in a reference cycle run in any
+    order. At interpreter exit nothing is destroyed; the driver reclaims the
+    device memory with the process."""
+
+    _deps = 0
+    _released = False
+    _parents = ()
+
+    def _adopt(self, *parents):
+        self._parents = tuple(p for p in parents if p is not None)
+        for p in self._parents:
+            p._deps += 1
+
+    def _drop(self):
+        if self._released and self._deps == 0 and getattr(self, "h", None):
+            self._free()
+            self.h = None
+            for p in self._parents:
+                p._deps -= 1
+                p._drop()
+
+    def __del__(self, _sys=sys):
+        if _sys.is_finalizing():
+            return
+        self._released = True
+        self._drop()
+
+
+class Context(_Native):
     """A device context (sb_ctx): one GPU, one CUDA stream."""
 
     def __init__(self, device=0):
@@ -152,10 +184,8 @@ class Context:
     def launch_count(self):
         return A.lib().sb_ctx_launch_count(self.h)
 
-    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
-        if getattr(self, "h", None):
-            _A.lib().sb_ctx_destroy(self.h)
-            self.h = None
+    def _free(self, _A=A):
+        _A.lib().sb_ctx_destroy(self.h)
 
 
 _DEFAULT = None
@@ -229,7 +259,7 @@ class DMatrix:
                           dtype=np.uint8)
 
 
-class GHistIndex:
+class GHistIndex(_Native):
     """HistCuts + GHistIndex resident on the device (sb_ghist)."""
 
     def __init__(self, dmat: DMatrix, max_bin=256, ctx: Context = None, device_ptr=None):
@@ -240,6 +270,7 @@ class GHistIndex:
                                         dmat.n_cols, A.ptr(ft, ctypes.c_uint8), dmat.missing, max_bin,
                                         ctypes.byref(h)))
         self.h = h
+        self._adopt(self.ctx)
         self._keep = ft
 
     @classmethod
@@ -253,6 +284,7 @@ class GHistIndex:
                                                A.ptr(ft, ctypes.c_uint8), missing, max_bin,
                                                ctypes.byref(h)))
         self.h = h
+        self._adopt(self.ctx)
         self._keep = ft
         return self
 
@@ -289,10 +321,8 @@ class GHistIndex:
         g[lb == 0xFFFF] = 0xFFFFFFFF
         return g
 
-    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
-        if getattr(self, "h", None):
-            _A.lib().sb_ghist_destroy(self.h)
-            self.h = None
+    def _free(self, _A=A):
+        _A.lib().sb_ghist_destroy(self.h)
 
 
 def _gpair(gpair):
@@ -355,13 +385,14 @@ class RegTree:
         return int((self.nodes["left"] == -1).sum())
 
 
-class BoostedModel:
+class BoostedModel(_Native):
     """The trained ensemble (learner/model.rs:34-54); arrays live on the host,
     a device copy is made on the first prediction."""
 
     def __init__(self, handle, ctx: Context):
         self.h = handle
         self.ctx = ctx
+        self._adopt(ctx)
 
     @classmethod
     def from_arrays(cls, node_off, nodes, cat_off, cats, base_score, num_class, n_features,
@@ -459,10 +490,27 @@ class BoostedModel:
                                             d.missing, A.ptr(out, ctypes.c_float)))
         return out.reshape(-1)
 
-    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
-        if getattr(self, "h", None):
-            _A.lib().sb_model_destroy(self.h)
-            self.h = None
+    def predict_leaf(self, d: DMatrix):
+        """Leaf node index per (row, tree), flat [n_rows * num_trees] u32
+        (predict_leaf, model.rs:330-341)."""
+        t = self.num_trees()
+        out = np.zeros((d.n_rows, t), np.uint32)
+        A.check(A.lib().sb_predict_leaf(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols, d.missing,
+                                        A.ptr(out, ctypes.c_uint32)))
+        return out.reshape(-1)
+
+    def predict_interactions(self, d: DMatrix):
+        """TreeSHAP interaction values, flat [n_rows][n_outputs][F+1][F+1]
+        (predict_interactions, shap.rs:395-509)."""
+        k = self.n_outputs()
+        w = d.n_cols + 1
+        out = np.zeros((d.n_rows, k, w, w), np.float32)
+        A.check(A.lib().sb_predict_interactions(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols,
+                                                d.missing, A.ptr(out, ctypes.c_float)))
+        return out.reshape(-1)
+
+    def _free(self, _A=A):
+        _A.lib().sb_model_destroy(self.h)
 
 
 def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Context = None):
@@ -550,7 +598,7 @@ class HistTreeBuilder:
         return (m, leaf) if return_row_leaf else m
 
 
-class Booster:
+class Booster(_Native):
     """The device-resident round loop (sb_booster): labels, margins,
     gradients and row lists stay on the GPU; `update(r)` runs r rounds."""
 
@@ -569,6 +617,7 @@ class Booster:
                                           A.ptr(bm, ctypes.c_float), ctypes.byref(h)))
         del keep
         self.h = h
+        self._adopt(self.ctx, ghist)
         self.n = lab.shape[0]
         self.k = params.num_class if params.objective.startswith("multi:") else 1
 
@@ -610,13 +659,11 @@ class Booster:
     def reset_stats(self):
         A.check(A.lib().sb_booster_stats_reset(self.h))
 
-    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
-        if getattr(self, "h", None):
-            _A.lib().sb_booster_destroy(self.h)
-            self.h = None
+    def _free(self, _A=A):
+        _A.lib().sb_booster_destroy(self.h)
 
 
-class Server:
+class Server(_Native):
     """The serving loop (sb_server): the model stays resident in HBM and margin
     / TreeSHAP requests from any thread are batched continuously on the
     device. `submit` returns a ticket; `wait` returns the request's output
@@ -631,6 +678,7 @@ class Server:
         h = ctypes.c_void_p()
         A.check(A.lib().sb_server_create(self.ctx.h, model.h, mem_bytes, n_slots, ctypes.byref(h)))
         self.h = h
+        self._adopt(self.ctx, model)
         self.k = model.n_outputs()
         self.f = model.info()[2]
         self._pending = {}
@@ -661,12 +709,10 @@ class Server:
         return {name: getattr(s, name) for name, _ in s._fields_}
 
     def close(self):
-        if getattr(self, "h", None):
-            A.check(A.lib().sb_server_destroy(self.h))
-            self.h = None
-            self._pending.clear()
+        """Finishes every queued request, then stops the loop."""
+        self._released = True
+        self._drop()
+        self._pending.clear()
 
-    def __del__(self, _A=A):  # bound at definition: module globals are gone at interpreter exit
-        if getattr(self, "h", None):
-            _A.lib().sb_server_destroy(self.h)
-            self.h = None
+    def _free(self, _A=A):
+        _A.check(_A.lib().sb_server_destroy(self.h))

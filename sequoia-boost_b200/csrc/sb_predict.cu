@@ -2,9 +2,10 @@
 //
 // Replaces BoostedModel::predict_margin_limited (learner/model.rs:231-285),
 // predict (:291-300, with pred_transform of objective/classification.rs:
-// :73-77 and multiclass.rs:93-99), and predict_contribs with tree_shap_cond,
-// extend_path, unwind_path, unwound_path_sum, node_mean_value
-// (learner/shap.rs:49-367).
+// :73-77 and multiclass.rs:93-99), predict_leaf (:330-341), predict_contribs
+// with tree_shap_cond, extend_path, unwind_path, unwound_path_sum,
+// node_mean_value (learner/shap.rs:49-367), and predict_interactions
+// (learner/shap.rs:395-509).
 //
 // Margins: phase 1 routes every (row, tree) pair in parallel and stores the
 // leaf value tree-major; phase 2 sums each (row, class) over its trees in
@@ -13,6 +14,7 @@
 // TreeSHAP: one thread per (row, tree) runs the path-dependent algorithm
 // iteratively (explicit DFS, one path snapshot per depth, hot child first)
 // in f64 and adds its contributions into a per-row f64 accumulator.
+#include <cmath>
 #include <cstring>
 #include <functional>
 
@@ -39,14 +41,18 @@ __device__ __forceinline__ bool is_missing_d(float v, float missing, bool miss_n
   return miss_nan ? isnan(v) : (v == missing);
 }
 
-// RegTree::leaf_id_with over a dense row (regtree.rs:213-242): leaf value.
-__device__ __forceinline__ float route(const PredDev& P, int t, const float* row, float missing,
-                                       bool miss_nan) {
+// RegTree::leaf_id_with over a dense row (regtree.rs:213-242): the leaf's
+// node index, and its packed node in *leaf.
+__device__ __forceinline__ int route_to_leaf(const PredDev& P, int t, const float* row, float missing,
+                                             bool miss_nan, int4* leaf) {
   const int4* nd = P.nodes + P.tree_off[t];
   int nid = 0;
   for (;;) {
     int4 x = __ldg(nd + nid);
-    if (x.z < 0) return __int_as_float(x.y);
+    if (x.z < 0) {
+      *leaf = x;
+      return nid;
+    }
     uint32_t ff = (uint32_t)x.x;
     float v = row[ff & NF_FEATURE];
     bool go_left;
@@ -65,6 +71,28 @@ __device__ __forceinline__ float route(const PredDev& P, int t, const float* row
     }
     nid = go_left ? x.z : x.w;
   }
+}
+
+// The leaf value of one tree for a dense row.
+__device__ __forceinline__ float route(const PredDev& P, int t, const float* row, float missing,
+                                       bool miss_nan) {
+  int4 x;
+  route_to_leaf(P, t, row, missing, miss_nan, &x);
+  return __int_as_float(x.y);
+}
+
+// predict_leaf (model.rs:330-341): out [n][T] leaf node ids, one thread per
+// (row, tree) with the tree index fastest, so the stores are coalesced and a
+// warp reads one row.
+__global__ void k_leaf_ids(PredDev P, const float* __restrict__ X, size_t n, int F, float missing,
+                           uint32_t* __restrict__ out) {
+  const size_t T = (size_t)P.n_trees;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * T) return;
+  const size_t r = i / T;
+  const int t = (int)(i - r * T);
+  int4 x;
+  out[i] = (uint32_t)route_to_leaf(P, t, X + r * F, missing, isnan(missing), &x);
 }
 
 // Margins in two phases. Phase 1 routes every (row, tree) pair in parallel
@@ -309,6 +337,202 @@ __global__ void k_shap_finish(const double* __restrict__ acc, const double* __re
   double v = acc[i];
   if (j == (size_t)F) v = bias[c];
   out[i] = (float)v;
+}
+
+// ------------------------------------------------- TreeSHAP interactions
+// predict_interactions (shap.rs:395-509) restated per root-to-leaf path, on
+// the same merged path elements as k_shap_paths. Conditioning the walk on
+// feature j (tree_shap_cond with condition +1 / -1) keeps j's splits off the
+// path and multiplies a leaf's weight by the condition fraction: o_j (the
+// row follows all of j's splits) when present, z_j (their cover fractions)
+// when absent. Paths without j give the same value both ways. So for a path
+// holding j as element m, the half-difference of the two runs is, for every
+// other element i:
+//     0.5 * (o_m - z_m) * UNWOUND_SUM(P \ m, i) * (o_i - z_i) * leaf,
+// added to M[j][f_i] and subtracted from M[j][j]; M[f][f] also gets the
+// ordinary contribution of the full path. A block takes IR rows (1 or 2)
+// and INTER_TREES trees of one class, accumulates the rows' (F+1)^2 matrices
+// in f32 shared memory (threads over (path, row), shared atomics), and adds
+// the non-zero cells into the f64 accumulator.
+constexpr int INTER_THREADS = 128;
+constexpr int INTER_TREES = 16;
+
+struct InterDev {
+  const PathEl* el;
+  const int* off;
+  const float* leaf;
+  const int* tree_path;  // [T + 1] first path of each tree
+  int T, K, F;
+  int rows_per_block;
+  unsigned row_blocks;
+  int groups_per_class;
+};
+
+// UNWOUND_SUM (unwound_path_sum, shap.rs:98-116) of an element with
+// one-fraction oo, zero-fraction zz (izz = 1 / zz) over weights w of a path
+// whose last index is ud.
+template <int MAXL>
+__device__ __forceinline__ double unwound_sum(const double* w, int ud, double oo, double zz, double izz) {
+  double wl = 0.0;
+#pragma unroll
+  for (int e = 0; e < MAXL; ++e)
+    if (e == ud) wl = w[e];
+  const double dn = (double)(ud + 1), idn = c_inv[ud + 1];
+  double next = wl, total = 0.0;
+#pragma unroll
+  for (int i = MAXL - 2; i >= 0; --i) {
+    if (i < ud) {
+      if (oo != 0.0) {
+        const double tmp = next * dn * c_inv[i + 1];
+        total += tmp;
+        next = w[i] - tmp * zz * (double)(ud - i) * idn;
+      } else if (zz != 0.0) {
+        total += w[i] * izz * dn * c_inv[ud - i];
+      }
+    }
+  }
+  return total;
+}
+
+template <int MAXL>
+__global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const float* __restrict__ X, size_t n,
+                                                              float missing, double* __restrict__ acc) {
+  extern __shared__ float mat[];  // [IR][W][W]
+  __shared__ int s_tree[INTER_TREES];
+  __shared__ int s_pre[INTER_TREES + 1];
+  const int F = P.F, W = F + 1, WW = W * W, IR = P.rows_per_block;
+  const unsigned rb = blockIdx.x % P.row_blocks;
+  const unsigned g = blockIdx.x / P.row_blocks;
+  const int c = (int)(g / (unsigned)P.groups_per_class), gi = (int)(g % (unsigned)P.groups_per_class);
+  const size_t r0 = (size_t)rb * IR;
+  for (int i = threadIdx.x; i < IR * WW; i += blockDim.x) mat[i] = 0.0f;
+  if (threadIdx.x == 0) {
+    int nt = 0, tot = 0;
+    s_pre[0] = 0;
+    for (int j = 0; j < INTER_TREES; ++j) {
+      const long long t = (long long)c + (long long)P.K * ((long long)gi * INTER_TREES + j);
+      if (t < P.T) {
+        s_tree[nt] = (int)t;
+        tot += P.tree_path[t + 1] - P.tree_path[t];
+        s_pre[++nt] = tot;
+      }
+    }
+    for (int j = nt + 1; j <= INTER_TREES; ++j) s_pre[j] = tot;
+  }
+  __syncthreads();
+  const int total = s_pre[INTER_TREES];
+  const bool miss_nan = isnan(missing);
+  for (int it = threadIdx.x; it < total * IR; it += blockDim.x) {
+    const int q = it / IR, ri = it - q * IR;
+    const size_t r = r0 + ri;
+    if (r >= n) continue;
+    int j = 0;
+    while (q >= s_pre[j + 1]) ++j;
+    const int p = P.tree_path[s_tree[j]] + (q - s_pre[j]);
+    const int e0 = P.off[p], L = P.off[p + 1] - e0;
+    const double leaf = (double)P.leaf[p];
+    const float* row = X + r * (size_t)F;
+    float* M = mat + ri * WW;
+    double z[MAXL], iz[MAXL], o[MAXL], w[MAXL];
+    int fe[MAXL];
+#pragma unroll
+    for (int e = 0; e < MAXL; ++e) {
+      fe[e] = 0;
+      z[e] = 1.0;
+      iz[e] = 1.0;
+      o[e] = 1.0;
+      if (e < L) {
+        const PathEl el = P.el[e0 + e];
+        fe[e] = el.f < 0 ? 0 : el.f;
+        z[e] = el.z;
+        iz[e] = el.inv_z;
+        if (el.f >= 0) {
+          const float v = __ldg(row + el.f);
+          const bool mis = miss_nan ? isnan(v) : v == missing;
+          o[e] = (mis ? el.miss_ok != 0 : (v >= el.lo && v < el.hi)) ? 1.0 : 0.0;
+        }
+      }
+    }
+    // the full path: ordinary contributions on the diagonal
+    w[0] = 1.0;
+#pragma unroll
+    for (int e = 1; e < MAXL; ++e) {
+      w[e] = 0.0;
+      if (e < L) {
+        const double inv = c_inv[e + 1];
+#pragma unroll
+        for (int i = e - 1; i >= 0; --i) {
+          const double pw = w[i];
+          w[i + 1] += o[e] * pw * (double)(i + 1) * inv;
+          w[i] = z[e] * pw * (double)(e - i) * inv;
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 1; e < MAXL; ++e)
+      if (e < L) {
+        const double v = unwound_sum<MAXL>(w, L - 1, o[e], z[e], iz[e]) * (o[e] - z[e]) * leaf;
+        if (v != 0.0) atomicAdd(M + fe[e] * W + fe[e], (float)v);
+      }
+    // conditioned on element m's feature: the path without m
+#pragma unroll
+    for (int m = 1; m < MAXL; ++m) {
+      if (m >= L) continue;
+      const double dm = o[m] - z[m];
+      if (dm == 0.0) continue;
+      double w2[MAXL];
+      w2[0] = 1.0;
+#pragma unroll
+      for (int k = 1; k < MAXL - 1; ++k) {
+        w2[k] = 0.0;
+        if (k < L - 1) {
+          const int sk = k < m ? k : k + 1;
+          const double inv = c_inv[k + 1];
+#pragma unroll
+          for (int i = k - 1; i >= 0; --i) {
+            const double pw = w2[i];
+            w2[i + 1] += o[sk] * pw * (double)(i + 1) * inv;
+            w2[i] = z[sk] * pw * (double)(k - i) * inv;
+          }
+        }
+      }
+      w2[MAXL - 1] = 0.0;
+      double dsum = 0.0;
+      const int row_m = fe[m] * W;
+#pragma unroll
+      for (int k = 1; k < MAXL - 1; ++k) {
+        if (k < L - 1) {
+          const int sk = k < m ? k : k + 1;
+          const double val =
+              0.5 * dm * unwound_sum<MAXL>(w2, L - 2, o[sk], z[sk], iz[sk]) * (o[sk] - z[sk]) * leaf;
+          if (val != 0.0) {
+            atomicAdd(M + row_m + fe[sk], (float)val);
+            dsum += val;
+          }
+        }
+      }
+      if (dsum != 0.0) atomicAdd(M + row_m + fe[m], (float)(-dsum));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < IR * WW; i += blockDim.x) {
+    const int ri = i / WW;
+    const size_t r = r0 + ri;
+    const float v = mat[i];
+    if (r < n && v != 0.0f) atomicAdd(acc + (r * P.K + c) * (size_t)WW + (i - ri * WW), (double)v);
+  }
+}
+
+// f64 accumulator -> f32 output; the [F][F] cell of each (row, class) is the
+// class's sum of tree expected values (no base score).
+__global__ void k_inter_finish(const double* __restrict__ acc, const double* __restrict__ bias, size_t n, int K,
+                               int F, float* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t W = (size_t)F + 1, WW = W * W;
+  if (i >= n * K * WW) return;
+  const size_t cell = i % WW;
+  const size_t c = (i / WW) % K;
+  out[i] = cell == (size_t)F * W + F ? (float)bias[c] : (float)acc[i];
 }
 
 int tree_depth(const HostTree& t) {
@@ -568,6 +792,72 @@ int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, f
   return SB_OK;
 }
 
+// Interaction values of n rows into d_out ([n][K][F+1][F+1] floats).
+int predict_interactions_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing,
+                                float* d_out) {
+  sb_ctx* ctx = m->ctx;
+  SB_TRY(model_upload(m));
+  SB_REQUIRE(m->dev.max_depth <= SHAP_MAXD, SB_ERR_UNSUPPORTED,
+             "TreeSHAP on the device supports trees up to depth %d (got %d)", SHAP_MAXD, m->dev.max_depth);
+  const int K = m->num_class >= 2 ? m->num_class : 1;
+  const int T = m->dev.n_trees;
+  const size_t W = F + 1, WW = W * W;
+  const size_t room = ctx->smem_optin > 1024 ? ctx->smem_optin - 1024 : 0;  // less the static shared memory
+  const int IR = 2 * WW * 4 <= room ? 2 : 1;
+  SB_REQUIRE((size_t)IR * WW * 4 <= room, SB_ERR_UNSUPPORTED,
+             "interaction values on the device support up to %d features",
+             (int)std::sqrt((double)(room / 4)) - 1);
+  const size_t smem = (size_t)IR * WW * 4;
+  SB_TRY(raise_smem_limit((const void*)k_shap_inter<5>, smem));
+  SB_TRY(raise_smem_limit((const void*)k_shap_inter<9>, smem));
+  SB_TRY(raise_smem_limit((const void*)k_shap_inter<SHAP_MAXD + 1>, smem));
+  // [F][F] cell per class: the sum of its trees' expected values (shap.rs:427-437)
+  std::vector<double> bias(K, 0.0);
+  for (int t = 0; t < T; ++t) bias[t % K] += node_mean_value(m->trees[t], 0);
+  DBuf<double> d_bias, acc;
+  SB_TRY(d_bias.alloc(ctx, K));
+  SB_CUDA(cudaMemcpyAsync(d_bias.p, bias.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (n == 0) return SB_OK;
+  // rows per pass: the f64 accumulator stays <= 256 MB
+  size_t chunk = std::max<size_t>((size_t)IR, (size_t)(256ull << 20) / ((size_t)K * WW * 8));
+  chunk = std::min(chunk, n);
+  SB_TRY(acc.alloc(ctx, chunk * K * WW));
+  InterDev P;
+  P.el = m->dev.path_el.p;
+  P.off = m->dev.path_off.p;
+  P.leaf = m->dev.path_leaf.p;
+  P.tree_path = m->dev.tree_path.p;
+  P.T = T;
+  P.K = K;
+  P.F = (int)F;
+  P.rows_per_block = IR;
+  const int per_class = (T + K - 1) / K;
+  P.groups_per_class = std::max(1, (per_class + INTER_TREES - 1) / INTER_TREES);
+  const int L = m->dev.max_path_len;
+  for (size_t r0 = 0; r0 < n; r0 += chunk) {
+    const size_t nb = std::min(chunk, n - r0);
+    SB_CUDA(cudaMemsetAsync(acc.p, 0, nb * K * WW * 8, ctx->stream));
+    P.row_blocks = (unsigned)((nb + IR - 1) / IR);
+    const uint64_t blocks = (uint64_t)P.row_blocks * (uint64_t)K * (uint64_t)P.groups_per_class;
+    SB_REQUIRE(blocks < (1ull << 31), SB_ERR_UNSUPPORTED, "interaction values: %llu blocks exceed one launch",
+               (unsigned long long)blocks);
+    if (T > 0) {
+      const float* X = d_X + r0 * F;
+      if (L <= 5)
+        SB_LAUNCH(ctx, k_shap_inter<5>, (unsigned)blocks, INTER_THREADS, smem, P, X, nb, missing, acc.p);
+      else if (L <= 9)
+        SB_LAUNCH(ctx, k_shap_inter<9>, (unsigned)blocks, INTER_THREADS, smem, P, X, nb, missing, acc.p);
+      else
+        SB_LAUNCH(ctx, k_shap_inter<SHAP_MAXD + 1>, (unsigned)blocks, INTER_THREADS, smem, P, X, nb, missing,
+                  acc.p);
+    }
+    const size_t tot = nb * K * WW;
+    SB_LAUNCH(ctx, k_inter_finish, (unsigned)((tot + 255) / 256), 256, 0, acc.p, d_bias.p, nb, K, (int)F,
+              d_out + r0 * K * WW);
+  }
+  return SB_OK;
+}
+
 // ---- batch launchers on an explicit stream with caller-owned buffers (used
 // by the serving loop; the model must be resident, see model_upload)
 
@@ -673,6 +963,56 @@ int sb_predict_contribs(sb_model* m, const float* X, size_t n_rows, size_t n_col
   SB_TRY(dout.alloc(ctx, n_rows * K * (n_cols + 1)));
   SB_CUDA(cudaMemcpyAsync(dX.p, X, dX.bytes(), cudaMemcpyHostToDevice, ctx->stream));
   SB_TRY(predict_contribs_device(m, dX.p, n_rows, n_cols, missing, dout.p));
+  SB_CUDA(cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+int sb_predict_leaf(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float missing, uint32_t* out) {
+  using namespace sb;
+  SB_REQUIRE(m && (out || n_rows == 0) && (X || n_rows == 0), SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(n_cols == (size_t)m->n_features, SB_ERR_DIMENSION,
+             "dimension mismatch: expected %d features, got %zu", m->n_features, n_cols);
+  sb_ctx* ctx = m->ctx;
+  SB_CUDA(cudaSetDevice(ctx->device));
+  SB_TRY(model_upload(m));
+  const size_t T = (size_t)m->dev.n_trees;
+  if (n_rows == 0 || T == 0) return SB_OK;
+  PredDev P;
+  P.nodes = m->dev.nodes.p;
+  P.cat_end = m->dev.cat_end.p;
+  P.tree_off = m->dev.tree_off.p;
+  P.cats = m->dev.cats.p;
+  P.weights = m->dev.weights.p;
+  P.n_trees = (int)T;
+  DBuf<float> dX;
+  DBuf<uint32_t> dout;
+  SB_TRY(dX.alloc(ctx, n_rows * n_cols));
+  SB_TRY(dout.alloc(ctx, n_rows * T));
+  SB_CUDA(cudaMemcpyAsync(dX.p, X, dX.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t tot = n_rows * T;
+  SB_REQUIRE((tot + 255) / 256 < (1ull << 31), SB_ERR_UNSUPPORTED, "predict_leaf: %zu outputs exceed one launch", tot);
+  SB_LAUNCH(ctx, k_leaf_ids, (unsigned)((tot + 255) / 256), 256, 0, P, dX.p, n_rows, (int)n_cols, missing, dout.p);
+  SB_CUDA(cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+int sb_predict_interactions(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float missing, float* out) {
+  using namespace sb;
+  SB_REQUIRE(m && (out || n_rows == 0) && (X || n_rows == 0), SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(n_cols == (size_t)m->n_features, SB_ERR_DIMENSION,
+             "dimension mismatch: expected %d features, got %zu", m->n_features, n_cols);
+  if (n_rows == 0) return SB_OK;
+  sb_ctx* ctx = m->ctx;
+  SB_CUDA(cudaSetDevice(ctx->device));
+  const int K = m->num_class >= 2 ? m->num_class : 1;
+  const size_t WW = (n_cols + 1) * (n_cols + 1);
+  DBuf<float> dX, dout;
+  SB_TRY(dX.alloc(ctx, n_rows * n_cols));
+  SB_TRY(dout.alloc(ctx, n_rows * K * WW));
+  SB_CUDA(cudaMemcpyAsync(dX.p, X, dX.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+  SB_TRY(predict_interactions_device(m, dX.p, n_rows, n_cols, missing, dout.p));
   SB_CUDA(cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
   SB_CUDA(cudaStreamSynchronize(ctx->stream));
   return SB_OK;

@@ -41,7 +41,8 @@ class OracleEngine:
         w = None if weights is None else np.asarray(weights, np.float32)
         return self.o.gradient(obj, preds, labels, w, k, spw)
 
-    def train(self, x, y, p, rounds, base_margin=None, ftypes=None, want_contribs=False):
+    def train(self, x, y, p, rounds, base_margin=None, ftypes=None, want_contribs=False,
+              want_interactions=False):
         r = self.o.train(x, y, p, rounds, base_margin=base_margin, ftypes=ftypes)
         arrays = r["model"].export()
         base = r["model"].base_score
@@ -55,6 +56,9 @@ class OracleEngine:
             out["contribs"] = self.o.predict_contribs(arrays, x, base, p.num_class)
             nodes = arrays[1]
             out["feature_unused"] = lambda f: not np.any((nodes["left"] != -1) & (nodes["split_feature"] == f))
+        if want_interactions:
+            out["interactions"] = self.o.predict_interactions(arrays, x, base, p.num_class)
+            out["base_score"] = base
         del k
         return out
 
@@ -102,7 +106,8 @@ class GpuEngine:
     def gradient(self, obj, preds, labels, weights, k, spw):
         raise NotImplementedError
 
-    def train(self, x, y, p, rounds, base_margin=None, ftypes=None, want_contribs=False):
+    def train(self, x, y, p, rounds, base_margin=None, ftypes=None, want_contribs=False,
+              want_interactions=False):
         d = self.sb.DMatrix(x, labels=y, base_margin=base_margin, feature_types=ftypes)
         m = self.sb.train(p, d, rounds, ctx=self.ctx)
         dx = self.sb.DMatrix(x, base_margin=base_margin)
@@ -111,4 +116,7 @@ class GpuEngine:
             out["contribs"] = m.predict_contribs(self.sb.DMatrix(x))
             nodes = m.export()[1]
             out["feature_unused"] = lambda f: not np.any((nodes["left"] != -1) & (nodes["split_feature"] == f))
+        if want_interactions:
+            out["interactions"] = m.predict_interactions(self.sb.DMatrix(x))
+            out["base_score"] = m.base_score()
         return out

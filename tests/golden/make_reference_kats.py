@@ -350,6 +350,19 @@ def main():
                   "params": {"objective": 0, "max_depth": 4, "eta": 0.3}, "tol": 1e-4,
                   "zero_feature": 3, "zero_tol": 1e-6})
 
+    # ---- TreeSHAP interaction values, learner/shap.rs:662-778: each feature
+    # row of a matrix sums to the feature's contribution (row consistency),
+    # the matrix sums to margin - base_score (efficiency), and the matrix is
+    # symmetric
+    cases.append({"name": "interactions_single_output", "ref": "learner/shap.rs:666-715",
+                  "kind": "interactions", "x": xs_, "y": ys_, "rounds": 30,
+                  "params": {"objective": 0, "max_depth": 4, "eta": 0.3},
+                  "tol_row": 1e-4, "tol_eff": 1e-4, "tol_sym": 1e-5})
+    cases.append({"name": "interactions_multiclass", "ref": "learner/shap.rs:716-778",
+                  "kind": "interactions", "x": xmc, "y": ymc, "rounds": 15,
+                  "params": {"objective": 4, "num_class": 3, "max_depth": 3, "eta": 0.3},
+                  "tol_row": 1e-4, "tol_eff": 1e-4, "tol_sym": 1e-5})
+
     with open(os.path.join(HERE, "reference_kats.json"), "w") as fh:
         json.dump({"generated_by": "tests/golden/make_reference_kats.py",
                    "source": "unit tests of pgarrett-scripps/sequoia-boost, crates/sequoia-boost/src",

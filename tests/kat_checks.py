@@ -228,4 +228,21 @@ def check_case(case, engine, Params):
             assert res["feature_unused"](f)
             assert np.max(np.abs(contribs[:, :, f])) < case["zero_tol"]
         return
+    if kind == "interactions":
+        x = xarr(case["x"])
+        y = np.asarray(case["y"], np.float32)
+        p = params_of(Params, case["params"])
+        res = engine.train(x, y, p, case["rounds"], want_contribs=True, want_interactions=True)
+        k = p.num_class if p.objective.startswith("multi:") else 1
+        w = x.shape[1] + 1
+        inter = res["interactions"].reshape(len(x), k, w, w).astype(np.float64)
+        contribs = res["contribs"].reshape(len(x), k, w).astype(np.float64)
+        margin = res["margin"].reshape(len(x), k).astype(np.float64)
+        row_err = np.max(np.abs(inter[:, :, :w - 1, :].sum(axis=3) - contribs[:, :, :w - 1]))
+        eff_err = np.max(np.abs(inter.sum(axis=(2, 3)) - (margin - res["base_score"])))
+        sym_err = np.max(np.abs(inter - inter.transpose(0, 1, 3, 2)))
+        assert row_err < case["tol_row"], (case["name"], row_err)
+        assert eff_err < case["tol_eff"], (case["name"], eff_err)
+        assert sym_err < case["tol_sym"], (case["name"], sym_err)
+        return
     raise AssertionError(f"unknown kind {kind}")
