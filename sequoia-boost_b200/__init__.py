@@ -6,7 +6,9 @@ src/lib.rs:86-97) over the C ABI in include/sb_gpu.h:
     TrainingParams   config/params.rs:76-373
     DMatrix          data/dmatrix.rs (dense f32 storage)
     train            learner/train.rs:107-113
-    BoostedModel     learner/model.rs (predict_margin, predict, predict_contribs)
+    BoostedModel     learner/model.rs (predict_margin, predict, predict_leaf,
+                     predict_contribs, predict_interactions, to/from_xgboost_json)
+    xgboost_json     model/xgboost_json.rs (XGBoost JSON model import/export)
     GHistIndex       data/ghist.rs + data/quantile.rs (device-resident cuts/bins)
     GpuBackend       tree/hist/mod.rs:31-45 (HistogramBackend: build, subtract)
     HistTreeBuilder  tree/builder/hist.rs:98-202

@@ -490,6 +490,34 @@ class BoostedModel(_Native):
                                             d.missing, A.ptr(out, ctypes.c_float)))
         return out.reshape(-1)
 
+    def objective_name(self):
+        from .xgboost_json import OBJECTIVE_NAMES
+        return OBJECTIVE_NAMES[self.info()[3]]
+
+    def to_xgboost_json(self):
+        """BoostedModel::to_xgboost_json (model.rs:435-437): the model in
+        XGBoost's JSON model schema (numeric splits only, as the reference)."""
+        from .xgboost_json import arrays_to_xgboost_json
+        base, k, f, _ = self.info()
+        off, nodes, _, _, _ = self.export()
+        return arrays_to_xgboost_json(off, nodes, base, k, f, self.objective_name())
+
+    @classmethod
+    def from_xgboost_json(cls, text, ctx: Context = None):
+        """BoostedModel::from_xgboost_json (model.rs:442-444)."""
+        from .xgboost_json import xgboost_json_to_arrays
+        off, nodes, coff, cats, base, k, f, obj = xgboost_json_to_arrays(text, NODE_DTYPE)
+        return cls.from_arrays(off, nodes, coff, cats, base, k, f, objective=obj, ctx=ctx)
+
+    def save_xgboost_json(self, path):
+        with open(path, "w") as fh:
+            fh.write(self.to_xgboost_json())
+
+    @classmethod
+    def load_xgboost_json(cls, path, ctx: Context = None):
+        with open(path) as fh:
+            return cls.from_xgboost_json(fh.read(), ctx=ctx)
+
     def predict_leaf(self, d: DMatrix):
         """Leaf node index per (row, tree), flat [n_rows * num_trees] u32
         (predict_leaf, model.rs:330-341)."""

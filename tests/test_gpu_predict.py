@@ -115,3 +115,30 @@ def test_margins_bit_exact_many_classes_and_trees(sb, ctx, orc):
     got = m.predict_margin(sb.DMatrix(x))
     want = orc.predict_margin(arrays, x, 0.25, K)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("objective", ["reg:squarederror", "binary:logistic", "multi:softprob"])
+def test_xgboost_json_roundtrip_on_device(sb, ctx, tmp_path, objective):
+    """BoostedModel.save_xgboost_json / load_xgboost_json (model.rs:446-455):
+    a numeric model comes back with the same trees; margins agree within
+    the base_score link's rounding (xgboost_json.rs:459-486)."""
+    x, _ = mixed_data(4000, 8, seed=11)
+    rng = np.random.default_rng(12)
+    kw = dict(objective=objective, max_depth=4, eta=0.3)
+    if objective == "multi:softprob":
+        kw["num_class"] = 3
+        y = rng.integers(0, 3, len(x)).astype(np.float32)
+    elif objective == "binary:logistic":
+        y = (np.nan_to_num(x[:, 0]) > 0).astype(np.float32)
+    else:
+        y = (np.nan_to_num(x[:, 0]) + rng.standard_normal(len(x))).astype(np.float32)
+    m = sb.train(sb.TrainingParams(**kw), sb.DMatrix(x, labels=y), 10, ctx=ctx)
+    path = tmp_path / "m.json"
+    m.save_xgboost_json(str(path))
+    r = sb.BoostedModel.load_xgboost_json(str(path), ctx=ctx)
+    assert r.num_trees() == m.num_trees() and r.objective_name() == objective
+    a, b = m.export(), r.export()
+    for key in ("left", "right", "split_feature", "split_cond", "leaf_value", "default_left"):
+        assert np.array_equal(a[1][key], b[1][key]), key
+    d = sb.DMatrix(x)
+    assert np.max(np.abs(m.predict(d) - r.predict(d))) < 1e-5
