@@ -370,14 +370,17 @@ struct InterDev {
 
 // UNWOUND_SUM (unwound_path_sum, shap.rs:98-116) of an element with
 // one-fraction oo, zero-fraction zz (izz = 1 / zz) over weights w of a path
-// whose last index is ud.
+// whose last index is ud. inv[k] = 1 / k: a shared-memory copy, because the
+// threads of a warp walk paths of different lengths and a constant-bank
+// read at divergent addresses is serialised.
 template <int MAXL>
-__device__ __forceinline__ double unwound_sum(const double* w, int ud, double oo, double zz, double izz) {
+__device__ __forceinline__ double unwound_sum(const double* w, int ud, double oo, double zz, double izz,
+                                              const double* inv) {
   double wl = 0.0;
 #pragma unroll
   for (int e = 0; e < MAXL; ++e)
     if (e == ud) wl = w[e];
-  const double dn = (double)(ud + 1), idn = c_inv[ud + 1];
+  const double dn = (double)(ud + 1), idn = inv[ud + 1];
   double next = wl, total = 0.0;
 #pragma unroll
   for (int i = MAXL - 2; i >= 0; --i) {
@@ -387,7 +390,7 @@ __device__ __forceinline__ double unwound_sum(const double* w, int ud, double oo
         total += tmp;
         next = w[i] - tmp * zz * (double)(ud - i) * idn;
       } else if (zz != 0.0) {
-        total += w[i] * izz * dn * c_inv[ud - i];
+        total += w[i] * izz * dn * inv[ud - i];
       }
     }
   }
@@ -400,12 +403,14 @@ __global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const 
   extern __shared__ float mat[];  // [IR][W][W]
   __shared__ int s_tree[INTER_TREES];
   __shared__ int s_pre[INTER_TREES + 1];
+  __shared__ double s_inv[32];
   const int F = P.F, W = F + 1, WW = W * W, IR = P.rows_per_block;
   const unsigned rb = blockIdx.x % P.row_blocks;
   const unsigned g = blockIdx.x / P.row_blocks;
   const int c = (int)(g / (unsigned)P.groups_per_class), gi = (int)(g % (unsigned)P.groups_per_class);
   const size_t r0 = (size_t)rb * IR;
   for (int i = threadIdx.x; i < IR * WW; i += blockDim.x) mat[i] = 0.0f;
+  if (threadIdx.x < 32) s_inv[threadIdx.x] = c_inv[threadIdx.x];
   if (threadIdx.x == 0) {
     int nt = 0, tot = 0;
     s_pre[0] = 0;
@@ -471,7 +476,7 @@ __global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const 
 #pragma unroll
     for (int e = 1; e < MAXL; ++e)
       if (e < L) {
-        const double v = unwound_sum<MAXL>(w, L - 1, o[e], z[e], iz[e]) * (o[e] - z[e]) * leaf;
+        const double v = unwound_sum<MAXL>(w, L - 1, o[e], z[e], iz[e], s_inv) * (o[e] - z[e]) * leaf;
         if (v != 0.0) atomicAdd(M + fe[e] * W + fe[e], (float)v);
       }
     // conditioned on element m's feature: the path without m
@@ -504,7 +509,7 @@ __global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const 
         if (k < L - 1) {
           const int sk = k < m ? k : k + 1;
           const double val =
-              0.5 * dm * unwound_sum<MAXL>(w2, L - 2, o[sk], z[sk], iz[sk]) * (o[sk] - z[sk]) * leaf;
+              0.5 * dm * unwound_sum<MAXL>(w2, L - 2, o[sk], z[sk], iz[sk], s_inv) * (o[sk] - z[sk]) * leaf;
           if (val != 0.0) {
             atomicAdd(M + row_m + fe[sk], (float)val);
             dsum += val;
