@@ -347,6 +347,38 @@ int sb_predict_leaf(sb_model* m, const float* X, size_t n_rows, size_t n_cols, f
 int sb_predict_interactions(sb_model* m, const float* X, size_t n_rows, size_t n_cols,
                             float missing, float* out);
 
+/* ------------------------------------------------ eval sets (train.rs) */
+/* train_with_eval's eval sets (learner/train.rs:121-140, 243-246, 319-379).
+ * sb_booster_eval_add uploads an eval set (X [n][n_cols], labels, optional
+ * weights, optional base_margin [n][K]) and starts its margin cache at
+ * init_margin (train.rs:240-241). sb_booster_eval adds the rounds grown since
+ * the last call into every cache (the same f32 sums as predict_margin) and
+ * writes out[e * n_metrics + j], metric j of eval set e, computed on the
+ * device after pred_transform (metric/mod.rs:37-262). Early stopping stays
+ * with the caller; sb_model_set_best_iteration records its pick. */
+enum {
+  SB_METRIC_RMSE = 0,     /* Rmse, metric/mod.rs:37-60 */
+  SB_METRIC_MAE = 1,      /* Mae, :62-85 */
+  SB_METRIC_LOGLOSS = 2,  /* LogLoss, :87-113 */
+  SB_METRIC_ERROR = 3,    /* ErrorRate, :115-142 */
+  SB_METRIC_MLOGLOSS = 4, /* MLogLoss, :194-226 (multi-output models) */
+  SB_METRIC_MERROR = 5    /* MError, :228-262 (multi-output models) */
+};
+#define SB_EVAL_MAX_METRICS 8
+#define SB_EVAL_MAX_CLASSES 64
+int sb_booster_eval_add(sb_booster* b, const float* X, size_t n_rows, size_t n_cols, float missing,
+                        const float* labels, const float* weights, const float* base_margin,
+                        int* eval_id);
+int sb_booster_eval(sb_booster* b, int n_metrics, const int* metrics, double* out);
+/* The margin cache of one eval set after the rounds grown so far: [n][K]. */
+int sb_booster_eval_margins(sb_booster* b, int eval_id, float* out);
+/* BoostedModel::set_best_iteration / best_iteration (model.rs:147-149,
+ * 209-211); -1 = none. sb_predict then uses (best_iteration + 1) * K trees
+ * (model.rs:213-219); sb_predict_margin's ntree_limit and the serving loop
+ * are not affected. */
+int sb_model_set_best_iteration(sb_model* m, int64_t best_iteration);
+int sb_model_best_iteration(const sb_model* m, int64_t* best_iteration);
+
 /* -------------------------------------------------------- serving loop */
 /* No counterpart in the reference (it predicts one call at a time). A tree
  * ensemble kept resident in HBM answers margin requests (the output of

@@ -30,10 +30,12 @@ from .api import (  # noqa: F401
     default_context,
     train,
     train_many,
+    train_with_eval,
 )
 from ._abi import SbError  # noqa: F401
 
 __all__ = [
     "BoostedModel", "Booster", "Context", "DMatrix", "GHistIndex", "GpuBackend",
     "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "train", "train_many",
+    "train_with_eval",
 ]

@@ -26,6 +26,8 @@ SB_OBJ_PSEUDOHUBER = 1
 SB_OBJ_LOGISTIC = 2
 SB_OBJ_SOFTMAX = 3
 SB_OBJ_SOFTPROB = 4
+SB_METRIC_RMSE, SB_METRIC_MAE, SB_METRIC_LOGLOSS, SB_METRIC_ERROR, SB_METRIC_MLOGLOSS, SB_METRIC_MERROR = range(6)
+SB_EVAL_MAX_METRICS = 8
 SB_GROW_DEPTHWISE = 0
 SB_GROW_LOSSGUIDE = 1
 SB_HIST_FP32 = 0
@@ -203,6 +205,11 @@ SIGNATURES = {
     "sb_predict_margin": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, SZ, F32P]),
     "sb_predict": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P]),
     "sb_predict_contribs": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
+    "sb_booster_eval_add": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P, F32P, ctypes.POINTER(I32)]),
+    "sb_booster_eval": (I32, [P, I32, ctypes.POINTER(I32), ctypes.POINTER(ctypes.c_double)]),
+    "sb_booster_eval_margins": (I32, [P, I32, F32P]),
+    "sb_model_set_best_iteration": (I32, [P, ctypes.c_int64]),
+    "sb_model_best_iteration": (I32, [P, ctypes.POINTER(ctypes.c_int64)]),
     "sb_predict_leaf": (I32, [P, F32P, SZ, SZ, ctypes.c_float, ctypes.POINTER(ctypes.c_uint32)]),
     "sb_predict_interactions": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
     "sb_server_create": (I32, [P, P, SZ, I32, ctypes.POINTER(P)]),

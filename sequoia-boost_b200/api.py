@@ -55,6 +55,7 @@ class TrainingParams:
     interaction_constraints: List[List[int]] = field(default_factory=list)
     hist_precision: str = "fp32"
     quantize_bits: int = 0
+    eval_metric: List[str] = field(default_factory=list)  # XGBoost `eval_metric` (params.rs:96-97)
 
     @staticmethod
     def builder():
@@ -124,7 +125,10 @@ class _ParamsBuilder:
         key = "lambda_" if name in ("lambda_", "reg_lambda") else name
 
         def setter(value):
-            setattr(self.params, key, value)
+            if key == "eval_metric":  # the builder appends (params.rs:342-345)
+                self.params.eval_metric = list(self.params.eval_metric) + [value]
+            else:
+                setattr(self.params, key, value)
             return self
         return setter
 
@@ -469,8 +473,20 @@ class BoostedModel(_Native):
                                           A.ptr(out, ctypes.c_float)))
         return out.reshape(-1)
 
+    def best_iteration(self):
+        """Early stopping's pick, or None (model.rs:209-211)."""
+        v = ctypes.c_int64()
+        A.check(A.lib().sb_model_best_iteration(self.h, ctypes.byref(v)))
+        return None if v.value < 0 else v.value
+
+    def set_best_iteration(self, it):
+        A.check(A.lib().sb_model_set_best_iteration(self.h, -1 if it is None else int(it)))
+
     def predict_margin(self, d: DMatrix):
-        return self.predict_margin_limited(d, 0)
+        """predict_margin (model.rs:222-226): (best_iteration + 1) * K trees
+        after early stopping, else all."""
+        it = self.best_iteration()
+        return self.predict_margin_limited(d, 0 if it is None else (it + 1) * self.n_outputs())
 
     def predict(self, d: DMatrix):
         k = self.n_outputs()
@@ -566,6 +582,87 @@ def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Co
     return BoostedModel(h, ctx)
 
 
+METRICS = {"rmse": A.SB_METRIC_RMSE, "mae": A.SB_METRIC_MAE, "logloss": A.SB_METRIC_LOGLOSS,
+           "error": A.SB_METRIC_ERROR, "mlogloss": A.SB_METRIC_MLOGLOSS, "merror": A.SB_METRIC_MERROR}
+# Objective::default_metric (regression.rs:47, :83, classification.rs:93, multiclass.rs:107)
+DEFAULT_METRIC = {"reg:squarederror": "rmse", "reg:linear": "rmse", "reg:pseudohubererror": "mae",
+                  "binary:logistic": "logloss", "reg:logistic": "logloss", "multi:softmax": "mlogloss",
+                  "multi:softprob": "mlogloss"}
+
+
+def _metric_id(name):
+    if name not in METRICS:
+        raise A.SbError(A.SB_ERR_UNSUPPORTED, f"metric `{name}` is not computed on the device "
+                                              f"(supported: {', '.join(METRICS)})")
+    return METRICS[name]
+
+
+@dataclass
+class RoundEval:
+    """One row of the evaluation history (train.rs:87-95)."""
+    iteration: int
+    scores: List[tuple]  # (eval set name, metric name, value)
+
+
+@dataclass
+class TrainResult:
+    """train_with_eval's result (train.rs:97-104)."""
+    model: "BoostedModel"
+    history: List[RoundEval]
+
+
+def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, evals=(),
+                    early_stopping_rounds: Optional[int] = None, ctx: Context = None):
+    """train_with_eval (learner/train.rs:121-140, loop :276-379): the rounds run
+    on the device-resident booster, each eval set keeps its margin cache on the
+    device, and only the metric values come back per round. Early stopping
+    watches the last metric of the last eval set; it stops after
+    `early_stopping_rounds` rounds without improvement and records the best
+    round, which `predict` / `predict_margin` then use."""
+    ctx = ctx or default_context()
+    if dtrain.labels is None:
+        raise A.SbError(A.SB_ERR_INVALID_ARG, "empty dataset: train: dtrain has no labels")
+    names = list(params.eval_metric) or [DEFAULT_METRIC.get(params.objective, "rmse")]
+    if len(names) > A.SB_EVAL_MAX_METRICS:
+        raise A.SbError(A.SB_ERR_INVALID_ARG, f"at most {A.SB_EVAL_MAX_METRICS} metrics")
+    for nm in names:
+        _metric_id(nm)
+    maximize = False  # none of the device metrics is maximised (metric/mod.rs:15-17)
+    gh = GHistIndex(dtrain, max_bin=params.max_bin, ctx=ctx)
+    k = params.num_class if params.objective.startswith("multi:") else 1
+    bm = None
+    if dtrain.base_margin is not None:
+        bm = np.ascontiguousarray(np.broadcast_to(dtrain.base_margin.reshape(dtrain.n_rows, -1),
+                                                  (dtrain.n_rows, k)).reshape(-1), np.float32)
+    b = Booster(gh, params, dtrain.labels, weights=dtrain.weights, base_margin=bm, ctx=ctx)
+    for d, _ in evals:
+        b.add_eval(d)
+    history = []
+    best_score = -math.inf if maximize else math.inf
+    best_iter, since = 0, 0
+    best_iteration = None
+    for rnd in range(num_boost_round):
+        b.update(1)
+        if not evals:
+            continue
+        vals = b.eval(names)
+        scores = [(evals[e][1], names[j], float(vals[e, j])) for e in range(len(evals)) for j in range(len(names))]
+        history.append(RoundEval(rnd, scores))
+        if early_stopping_rounds is not None:
+            last = scores[-1][2]
+            if (last > best_score) if maximize else (last < best_score):
+                best_score, best_iter, since = last, rnd, 0
+            else:
+                since += 1
+                if since >= early_stopping_rounds:
+                    best_iteration = best_iter
+                    break
+    m = b.model()
+    if best_iteration is not None:
+        m.set_best_iteration(best_iteration)
+    return TrainResult(m, history)
+
+
 def train_many(jobs, n_streams=16, ctx: Context = None):
     """Trains independent jobs together on the GPU (sb_train_many): `jobs` is
     a list of (TrainingParams, DMatrix with labels, num_boost_round). Returns
@@ -648,6 +745,7 @@ class Booster(_Native):
         self._adopt(self.ctx, ghist)
         self.n = lab.shape[0]
         self.k = params.num_class if params.objective.startswith("multi:") else 1
+        self._eval_rows = []
 
     def update(self, rounds=1):
         A.check(A.lib().sb_booster_update(self.h, rounds))
@@ -671,6 +769,38 @@ class Booster(_Native):
         h = ctypes.c_void_p()
         A.check(A.lib().sb_booster_model(self.h, ctypes.byref(h)))
         return BoostedModel(h, self.ctx)
+
+    def add_eval(self, d: DMatrix):
+        """Attaches an eval set (its rows, labels, weights and margin cache go
+        to the device); returns its index."""
+        if d.labels is None:
+            raise A.SbError(A.SB_ERR_INVALID_ARG, "an eval set needs labels")
+        bm = None
+        if d.base_margin is not None:
+            bm = np.ascontiguousarray(np.broadcast_to(d.base_margin.reshape(d.n_rows, -1),
+                                                      (d.n_rows, self.k)).reshape(-1), np.float32)
+        eid = ctypes.c_int()
+        A.check(A.lib().sb_booster_eval_add(self.h, A.ptr(d.data, ctypes.c_float), d.n_rows, d.n_cols, d.missing,
+                                            A.ptr(d.labels, ctypes.c_float), A.ptr(d.weights, ctypes.c_float),
+                                            A.ptr(bm, ctypes.c_float), ctypes.byref(eid)))
+        self._eval_rows.append(d.n_rows)
+        return eid.value
+
+    def eval(self, metrics):
+        """Metric values [n_eval_sets][len(metrics)] after the rounds grown so
+        far; `metrics` are names (rmse, mae, logloss, error, mlogloss, merror)."""
+        ids = [_metric_id(m) for m in metrics]
+        n_e = len(self._eval_rows)
+        out = np.zeros((max(n_e, 1), max(len(ids), 1)), np.float64)
+        arr = (ctypes.c_int * max(len(ids), 1))(*ids)
+        A.check(A.lib().sb_booster_eval(self.h, len(ids), arr, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out[:n_e, :len(ids)]
+
+    def eval_margins(self, eval_id):
+        """The margin cache of an eval set, [n_rows][n_outputs]."""
+        out = np.zeros((self._eval_rows[eval_id], self.k), np.float32)
+        A.check(A.lib().sb_booster_eval_margins(self.h, eval_id, A.ptr(out, ctypes.c_float)))
+        return out
 
     def set_timing(self, on=True):
         A.check(A.lib().sb_booster_set_timing(self.h, 1 if on else 0))

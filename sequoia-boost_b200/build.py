@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsb_gpu.so")
-SOURCES = ["sb_core.cu", "sb_bin.cu", "sb_hist.cu", "sb_grow.cu", "sb_predict.cu", "sb_static.cu", "sb_serve.cu", "sb_jobs.cu"]
+SOURCES = ["sb_core.cu", "sb_bin.cu", "sb_hist.cu", "sb_grow.cu", "sb_predict.cu", "sb_static.cu", "sb_serve.cu", "sb_jobs.cu", "sb_eval.cu"]
 HEADERS = ["sb_internal.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

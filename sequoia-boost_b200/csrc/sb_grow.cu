@@ -20,6 +20,7 @@
 // All frontier nodes of all K class trees are processed by each launch.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 
 #include "sb_internal.cuh"
 
@@ -1608,6 +1609,7 @@ struct sb_booster {
   std::vector<cudaEvent_t> ev;
   std::vector<int> ev_kind;  // 0 = hist pair, 1 = round pair
   std::vector<double> ev_bytes;
+  std::vector<std::unique_ptr<sb::EvalSet>> evals;  // eval sets (sb_booster_eval_add)
 };
 
 namespace sb {
@@ -2153,6 +2155,23 @@ int booster_export(const sb_booster* b, sb_model* m) {
   m->objective = b->p.objective;
   return SB_OK;
 }
+
+int booster_trees(const sb_booster* b, BoosterTrees* v) {
+  v->ctx = b->ctx;
+  v->nodes = b->d_out_nodes.p;
+  v->cats = b->S.cat_cap ? b->d_out_cats.p : nullptr;
+  v->maxn = b->maxn;
+  v->cat_cap = b->S.cat_cap;
+  v->K = b->K;
+  v->rounds_done = b->rounds_done;
+  v->base_score = b->base_score;
+  v->objective = b->p.objective;
+  v->num_class = b->p.num_class;
+  v->n_features = b->g->F;
+  return SB_OK;
+}
+
+std::vector<std::unique_ptr<EvalSet>>& booster_evals(sb_booster* b) { return b->evals; }
 
 // Folds a pending tree's leaf values into the margins before the host reads them.
 int booster_flush_delta(const sb_booster* b) {

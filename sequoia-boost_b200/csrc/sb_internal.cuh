@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -229,6 +230,7 @@ struct sb_model {
   int num_class = 0;
   int n_features = 0;
   int objective = 0;
+  int64_t best_iteration = -1;  // early stopping's pick (-1: none), model.rs:41
   bool dev_valid = false;
   sb::DevEnsemble dev;
 };
@@ -237,6 +239,31 @@ namespace sb {
 
 int n_outputs(int objective, int num_class);
 int model_upload(sb_model* m);
+
+// The trees a booster has grown so far, as they sit on the device: tree
+// t = round * K + class at nodes[t * maxn ..], its categories at
+// cats[t * cat_cap ..] (leaf values already scaled by eta).
+struct BoosterTrees {
+  sb_ctx* ctx;
+  const sb_node* nodes;
+  const uint32_t* cats;  // null when no tree can hold categorical splits
+  int maxn, cat_cap, K, rounds_done;
+  float base_score;      // margin space
+  int objective, num_class;
+  size_t n_features;
+};
+
+// An eval set attached to a booster (train_impl's `evals`, train.rs:243-246):
+// its rows, labels, weights and incremental margin cache stay on the device.
+struct EvalSet {
+  DBuf<float> X, labels, weights, margin, preds;
+  size_t n = 0;
+  float missing = NAN;
+  int rounds_in_margin = 0;  // rounds already added into `margin`
+};
+
+int booster_trees(const sb_booster* b, BoosterTrees* v);
+std::vector<std::unique_ptr<EvalSet>>& booster_evals(sb_booster* b);
 
 // ---------------------------------------------------- FP64 split math
 // Written with explicit round-to-nearest intrinsics so that no FMA
@@ -303,6 +330,34 @@ __host__ __device__ __forceinline__ uint32_t f32_as_u32(float v) {
   if (!(v > 0.0f)) return 0u;
   if (v >= 4294967296.0f) return 0xFFFFFFFFu;
   return (uint32_t)v;
+}
+
+// Objective::pred_transform over one row of K margins, in place: the
+// logistic sigmoid (classification.rs:73-77) or the softmax
+// (multiclass.rs:93-99), in f32 with explicit rounding; the identity for the
+// regression objectives.
+__device__ __forceinline__ void pred_transform_row(float* row, int K, int objective) {
+  if (objective == SB_OBJ_LOGISTIC) {
+    const float x = row[0];
+    float p;
+    if (x >= 0.0f) p = __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-x)));
+    else {
+      const float e = expf(x);
+      p = __fdiv_rn(e, __fadd_rn(1.0f, e));
+    }
+    row[0] = p;
+  } else if ((objective == SB_OBJ_SOFTMAX || objective == SB_OBJ_SOFTPROB) && K > 1) {
+    float mx = -INFINITY;
+    for (int c = 0; c < K; ++c)
+      if (row[c] > mx) mx = row[c];
+    float sum = 0.0f;
+    for (int c = 0; c < K; ++c) {
+      row[c] = expf(__fsub_rn(row[c], mx));
+      sum = __fadd_rn(sum, row[c]);
+    }
+    const float inv = __fdiv_rn(1.0f, sum);
+    for (int c = 0; c < K; ++c) row[c] = __fmul_rn(row[c], inv);
+  }
 }
 
 // Power-of-two exponent of the fixed-point scale: q = rint(x * 2^s) keeps

@@ -182,28 +182,7 @@ int margins(sb_ctx* ctx, cudaStream_t st, const PredDev& P, const float* d_X, si
 __global__ void k_transform(float* __restrict__ v, size_t n, int K, int objective) {
   size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
-  if (objective == SB_OBJ_LOGISTIC) {
-    float x = v[r];
-    float p;
-    if (x >= 0.0f) p = __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-x)));
-    else {
-      float e = expf(x);
-      p = __fdiv_rn(e, __fadd_rn(1.0f, e));
-    }
-    v[r] = p;
-  } else if ((objective == SB_OBJ_SOFTMAX || objective == SB_OBJ_SOFTPROB) && K > 1) {
-    float* row = v + r * K;
-    float mx = -INFINITY;
-    for (int c = 0; c < K; ++c)
-      if (row[c] > mx) mx = row[c];
-    float sum = 0.0f;
-    for (int c = 0; c < K; ++c) {
-      row[c] = expf(__fsub_rn(row[c], mx));
-      sum = __fadd_rn(sum, row[c]);
-    }
-    float inv = __fdiv_rn(1.0f, sum);
-    for (int c = 0; c < K; ++c) row[c] = __fmul_rn(row[c], inv);
-  }
+  pred_transform_row(v + r * K, K, objective);
 }
 
 // ------------------------------------------------------------- TreeSHAP
@@ -946,7 +925,10 @@ int sb_predict(sb_model* m, const float* X, size_t n_rows, size_t n_cols, float 
     SB_TRY(dbm.alloc(ctx, n_rows * K));
     SB_CUDA(cudaMemcpyAsync(dbm.p, base_margin, dbm.bytes(), cudaMemcpyHostToDevice, ctx->stream));
   }
-  SB_TRY(predict_margin_device(m, dX.p, n_rows, n_cols, missing, dbm.p, 1, 0, dout.p));
+  // predict uses the effective tree count: (best_iteration + 1) * K after
+  // early stopping, else all trees (model.rs:213-219)
+  const size_t limit = m->best_iteration >= 0 ? (size_t)(m->best_iteration + 1) * K : 0;
+  SB_TRY(predict_margin_device(m, dX.p, n_rows, n_cols, missing, dbm.p, 1, limit, dout.p));
   SB_LAUNCH(ctx, k_transform, (unsigned)((n_rows + 255) / 256), 256, 0, dout.p, n_rows, K, m->objective);
   SB_CUDA(cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
   SB_CUDA(cudaStreamSynchronize(ctx->stream));
