@@ -627,7 +627,6 @@ def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: in
         raise A.SbError(A.SB_ERR_INVALID_ARG, f"at most {A.SB_EVAL_MAX_METRICS} metrics")
     for nm in names:
         _metric_id(nm)
-    maximize = False  # none of the device metrics is maximised (metric/mod.rs:15-17)
     gh = GHistIndex(dtrain, max_bin=params.max_bin, ctx=ctx)
     k = params.num_class if params.objective.startswith("multi:") else 1
     bm = None
@@ -638,9 +637,8 @@ def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: in
     for d, _ in evals:
         b.add_eval(d)
     history = []
-    best_score = -math.inf if maximize else math.inf
-    best_iter, since = 0, 0
-    best_iteration = None
+    # none of the device metrics is maximised (metric/mod.rs:15-17)
+    stop = EarlyStopping(early_stopping_rounds, maximize=False)
     for rnd in range(num_boost_round):
         b.update(1)
         if not evals:
@@ -648,19 +646,39 @@ def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: in
         vals = b.eval(names)
         scores = [(evals[e][1], names[j], float(vals[e, j])) for e in range(len(evals)) for j in range(len(names))]
         history.append(RoundEval(rnd, scores))
-        if early_stopping_rounds is not None:
-            last = scores[-1][2]
-            if (last > best_score) if maximize else (last < best_score):
-                best_score, best_iter, since = last, rnd, 0
-            else:
-                since += 1
-                if since >= early_stopping_rounds:
-                    best_iteration = best_iter
-                    break
+        if stop.update(rnd, scores[-1][2]):
+            break
     m = b.model()
-    if best_iteration is not None:
-        m.set_best_iteration(best_iteration)
+    if stop.best_iteration is not None:
+        m.set_best_iteration(stop.best_iteration)
     return TrainResult(m, history)
+
+
+class EarlyStopping:
+    """train_impl's early-stopping bookkeeping (train.rs:264-271, 350-377): the
+    last metric of the last eval set must improve strictly within `patience`
+    rounds; on a stop, `best_iteration` is the round of the best value."""
+
+    def __init__(self, patience, maximize=False):
+        self.patience = patience
+        self.maximize = maximize
+        self.best_score = -math.inf if maximize else math.inf
+        self.best_round = 0
+        self.since = 0
+        self.best_iteration = None
+
+    def update(self, rnd, value):
+        """Records round `rnd`'s value; True when training must stop."""
+        if self.patience is None:
+            return False
+        if (value > self.best_score) if self.maximize else (value < self.best_score):
+            self.best_score, self.best_round, self.since = value, rnd, 0
+            return False
+        self.since += 1
+        if self.since >= self.patience:
+            self.best_iteration = self.best_round
+            return True
+        return False
 
 
 def train_many(jobs, n_streams=16, ctx: Context = None):
