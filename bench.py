@@ -22,6 +22,7 @@ the same workload.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -262,13 +263,32 @@ def serving_leg(sb, ctx, args, torch):
         wall = max(time.perf_counter() - t0, 1e-9)
         return _latency_summary(lat, rows, kinds, wall)
 
+    def run_prediction():
+        """Whole-call throughput of the other prediction entry points on the
+        same model (host buffers, copies included), best of 3."""
+        out = {}
+        for name, rows, fn in (("contribs_rows_per_s", 4096, model.predict_contribs),
+                               ("interactions_rows_per_s", 128, model.predict_interactions),
+                               ("leaf_rows_per_s", 65536, model.predict_leaf)):
+            d = sb.DMatrix(pool[:rows])
+            fn(d)
+            best = math.inf
+            for _ in range(3):
+                t0 = time.perf_counter()
+                fn(d)
+                best = min(best, time.perf_counter() - t0)
+            out[name] = rows / best
+        return out
+
     batched = run_batched()
     plain = run_plain()
+    pred = run_prediction()
     return {"workload": f"1000-tree depth-8 binary:logistic ensemble (trained on {n} binary_mixed rows), "
                         f"{N} requests, Poisson {args.serve_rate:g} req/s, rows log-uniform [1, 65536], "
                         "10% NaN, 90% margin / 10% TreeSHAP",
             "batched": batched, "plain_gpu": plain,
-            "requests_margin": int((kinds == 0).sum()), "requests_contribs": int(kinds.sum())}
+            "requests_margin": int((kinds == 0).sum()), "requests_contribs": int(kinds.sum()),
+            "prediction": pred}
 
 
 def run_reference(args):
