@@ -458,11 +458,23 @@ __global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const 
         const double v = unwound_sum<MAXL>(w, L - 1, o[e], z[e], iz[e], s_inv) * (o[e] - z[e]) * leaf;
         if (v != 0.0) atomicAdd(M + fe[e] * W + fe[e], (float)v);
       }
-    // conditioned on element m's feature: the path without m
+    // conditioned on element m's feature: the path without m. The m loop is
+    // not unrolled: unrolling all three loop levels made the kernel larger
+    // than the instruction cache (ncu: "no instruction" was the top stall).
+    // Element m's values are picked with static indices, so the arrays stay
+    // in registers.
+#pragma unroll 1
+    for (int m = 1; m < L; ++m) {
+      double zm = 1.0, om = 1.0;
+      int fm = 0;
 #pragma unroll
-    for (int m = 1; m < MAXL; ++m) {
-      if (m >= L) continue;
-      const double dm = o[m] - z[m];
+      for (int e = 1; e < MAXL; ++e)
+        if (e == m) {
+          zm = z[e];
+          om = o[e];
+          fm = fe[e];
+        }
+      const double dm = om - zm;
       if (dm == 0.0) continue;
       double w2[MAXL];
       w2[0] = 1.0;
@@ -470,32 +482,35 @@ __global__ void __launch_bounds__(INTER_THREADS) k_shap_inter(InterDev P, const 
       for (int k = 1; k < MAXL - 1; ++k) {
         w2[k] = 0.0;
         if (k < L - 1) {
-          const int sk = k < m ? k : k + 1;
+          const bool after = k >= m;  // reduced position k holds element k + 1
+          const double ok = after ? o[k + 1] : o[k], zk = after ? z[k + 1] : z[k];
           const double inv = c_inv[k + 1];
 #pragma unroll
           for (int i = k - 1; i >= 0; --i) {
             const double pw = w2[i];
-            w2[i + 1] += o[sk] * pw * (double)(i + 1) * inv;
-            w2[i] = z[sk] * pw * (double)(k - i) * inv;
+            w2[i + 1] += ok * pw * (double)(i + 1) * inv;
+            w2[i] = zk * pw * (double)(k - i) * inv;
           }
         }
       }
       w2[MAXL - 1] = 0.0;
       double dsum = 0.0;
-      const int row_m = fe[m] * W;
+      const int row_m = fm * W;
 #pragma unroll
       for (int k = 1; k < MAXL - 1; ++k) {
         if (k < L - 1) {
-          const int sk = k < m ? k : k + 1;
-          const double val =
-              0.5 * dm * unwound_sum<MAXL>(w2, L - 2, o[sk], z[sk], iz[sk], s_inv) * (o[sk] - z[sk]) * leaf;
+          const bool after = k >= m;
+          const double ok = after ? o[k + 1] : o[k], zk = after ? z[k + 1] : z[k];
+          const double izk = after ? iz[k + 1] : iz[k];
+          const int fk = after ? fe[k + 1] : fe[k];
+          const double val = 0.5 * dm * unwound_sum<MAXL>(w2, L - 2, ok, zk, izk, s_inv) * (ok - zk) * leaf;
           if (val != 0.0) {
-            atomicAdd(M + row_m + fe[sk], (float)val);
+            atomicAdd(M + row_m + fk, (float)val);
             dsum += val;
           }
         }
       }
-      if (dsum != 0.0) atomicAdd(M + row_m + fe[m], (float)(-dsum));
+      if (dsum != 0.0) atomicAdd(M + row_m + fm, (float)(-dsum));
     }
   }
   __syncthreads();
