@@ -323,6 +323,21 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms, dist, device=None):
+    """The job's time for a step range: the slowest rank's device time."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, n, steps, ms):
+    """Whole-job Mrow-rounds/s: every rank's replica trains n rows per round."""
+    return world * n * steps / (ms / 1e3) / 1e6
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -373,11 +388,9 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, f"cuda:{local}")
         dist.barrier()
-    value = world * n * args.steps / (ms / 1e3) / 1e6
+    value = job_value(world, n, args.steps, ms)
 
     # roofline of the histogram kernel: algorithmic bytes / device time
     b.set_timing(True)
