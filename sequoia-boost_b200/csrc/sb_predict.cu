@@ -333,7 +333,7 @@ __global__ void k_shap_finish(const double* __restrict__ acc, const double* __re
 // and INTER_TREES trees of one class, accumulates the rows' (F+1)^2 matrices
 // in f32 shared memory (threads over (path, row), shared atomics), and adds
 // the non-zero cells into the f64 accumulator.
-constexpr int INTER_THREADS = 128;
+constexpr int INTER_THREADS = 256;
 constexpr int INTER_TREES = 16;
 
 struct InterDev {
