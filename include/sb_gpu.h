@@ -248,6 +248,11 @@ int sb_booster_update(sb_booster* b, int n_rounds);
 int sb_booster_margins(const sb_booster* b, float* out);
 /* Gradient pairs of the last round, class-major [K][n] (host). */
 int sb_booster_gradients(const sb_booster* b, sb_gradpair* out);
+/* Replaces the booster's margins [n][K] (host buffer) before the next round,
+ * which then takes its gradients from them; the last tree's leaf values are
+ * not added on top. DART's rounds (train.rs:384-456) take their gradients
+ * from the ensemble minus the dropped trees this way. */
+int sb_booster_set_margins(sb_booster* b, const float* margins);
 /* Rows sampled in round `round` (host, n bytes: 1 = in the subset). */
 int sb_booster_row_mask(const sb_booster* b, uint64_t round, uint8_t* out);
 /* Copies the trees grown so far into a new model handle. */

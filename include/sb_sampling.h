@@ -64,6 +64,14 @@ SB_HD uint64_t sb_node_key(uint64_t tree_key, uint64_t nid) {
   return sb_mix64(tree_key ^ sb_mix64(nid + 0x6E6F6465ULL));
 }
 
+/* Key of a DART round's dropout draws (train.rs:397-425): a sequential
+ * stream seeded with it draws skip (u01 < skip_drop), then one u01 per
+ * existing tree (dropped if < rate_drop), then, when none was dropped, the
+ * one tree to drop (bounded draw). The host side of the DART loop uses it. */
+SB_HD uint64_t sb_dart_key(uint64_t seed, uint64_t round) {
+  return sb_mix64(seed ^ sb_mix64(round + 0x0DA27ULL) ^ 0x64617274ULL);
+}
+
 /* Sequential SplitMix64 stream. */
 typedef struct sb_splitmix { uint64_t s; } sb_splitmix;
 

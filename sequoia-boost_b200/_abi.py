@@ -205,6 +205,7 @@ SIGNATURES = {
     "sb_predict_margin": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, SZ, F32P]),
     "sb_predict": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P]),
     "sb_predict_contribs": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P]),
+    "sb_booster_set_margins": (I32, [P, F32P]),
     "sb_booster_eval_add": (I32, [P, F32P, SZ, SZ, ctypes.c_float, F32P, F32P, F32P, ctypes.POINTER(I32)]),
     "sb_booster_eval": (I32, [P, I32, ctypes.POINTER(I32), ctypes.POINTER(ctypes.c_double)]),
     "sb_booster_eval_margins": (I32, [P, I32, F32P]),

@@ -56,6 +56,9 @@ class TrainingParams:
     hist_precision: str = "fp32"
     quantize_bits: int = 0
     eval_metric: List[str] = field(default_factory=list)  # XGBoost `eval_metric` (params.rs:96-97)
+    booster: str = "gbtree"  # "gbtree" | "dart" (params.rs:79; gblinear is not built)
+    rate_drop: float = 0.0   # DART (params.rs:143-146)
+    skip_drop: float = 0.0
 
     @staticmethod
     def builder():
@@ -112,6 +115,13 @@ class TrainingParams:
     def validate(self):
         p, _keep = self.to_c()
         A.check(A.lib().sb_train_params_validate(ctypes.byref(p)))
+        if self.booster not in ("gbtree", "dart"):
+            raise A.SbError(A.SB_ERR_UNSUPPORTED if self.booster == "gblinear" else A.SB_ERR_INVALID_ARG,
+                            f"booster `{self.booster}` is not available (gbtree, dart)")
+        for name in ("rate_drop", "skip_drop"):  # params.rs:244-245
+            v = getattr(self, name)
+            if not (0.0 <= v <= 1.0):
+                raise A.SbError(A.SB_ERR_INVALID_ARG, f"invalid parameter {name}={v}: must be in [0, 1]")
         return self
 
 
@@ -563,6 +573,9 @@ def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Co
     ctx = ctx or default_context()
     if dtrain.labels is None:
         raise A.SbError(A.SB_ERR_INVALID_ARG, "empty dataset: train: dtrain has no labels")
+    if params.booster != "gbtree":
+        params.validate()
+        return _train_dart(params, dtrain, num_boost_round, ctx)
     p, keep = params.to_c()
     ft = dtrain._ftypes()
     bm = None
@@ -622,6 +635,11 @@ def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: in
     ctx = ctx or default_context()
     if dtrain.labels is None:
         raise A.SbError(A.SB_ERR_INVALID_ARG, "empty dataset: train: dtrain has no labels")
+    if params.booster != "gbtree":
+        params.validate()
+        if evals:
+            raise A.SbError(A.SB_ERR_UNSUPPORTED, "eval sets with booster=dart are not built")
+        return TrainResult(_train_dart(params, dtrain, num_boost_round, ctx), [])
     names = list(params.eval_metric) or [DEFAULT_METRIC.get(params.objective, "rmse")]
     if len(names) > A.SB_EVAL_MAX_METRICS:
         raise A.SbError(A.SB_ERR_INVALID_ARG, f"at most {A.SB_EVAL_MAX_METRICS} metrics")
@@ -652,6 +670,86 @@ def train_with_eval(params: TrainingParams, dtrain: DMatrix, num_boost_round: in
     if stop.best_iteration is not None:
         m.set_best_iteration(stop.best_iteration)
     return TrainResult(m, history)
+
+
+_M64 = (1 << 64) - 1
+
+
+def _mix64(z):
+    """sb_mix64 of include/sb_sampling.h."""
+    z = (z + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def dart_dropout(seed, rnd, existing, rate_drop, skip_drop):
+    """DART's dropout set for round `rnd` over the `existing` trees
+    (train.rs:397-425): skipped with probability skip_drop, else each tree
+    with probability rate_drop, and at least one. The draws come from the
+    SplitMix64 stream of sb_dart_key (include/sb_sampling.h), not rand 0.8."""
+    s = _mix64((seed & _M64) ^ _mix64((rnd + 0x0DA27) & _M64) ^ 0x64617274)
+
+    def nxt():
+        nonlocal s
+        x = _mix64(s)
+        s = (s + 0x9E3779B97F4A7C15) & _M64
+        return x
+
+    def u01():
+        return (nxt() >> 11) * (1.0 / 9007199254740992.0)
+
+    if u01() < skip_drop or existing == 0:
+        return []
+    dropped = [i for i in range(existing) if u01() < rate_drop]
+    if not dropped:
+        dropped = [(nxt() * existing) >> 64]
+    return dropped
+
+
+def _train_dart(params, dtrain, num_boost_round, ctx):
+    """dart_round (learner/train.rs:384-456) over the device booster: per
+    round, the margins of the ensemble minus the dropout set are predicted on
+    the device (tree weights, dropped trees at 0) and handed to the booster,
+    whose next round grows the K new trees from their gradients; the new
+    trees get weight 1/(k+1) and the k dropped trees are scaled by k/(k+1)."""
+    k_out = params.num_class if params.objective.startswith("multi:") else 1
+    gh = GHistIndex(dtrain, max_bin=params.max_bin, ctx=ctx)
+    bm = None
+    if dtrain.base_margin is not None:
+        bm = np.ascontiguousarray(np.broadcast_to(dtrain.base_margin.reshape(dtrain.n_rows, -1),
+                                                  (dtrain.n_rows, k_out)), np.float32)
+    b = Booster(gh, params, dtrain.labels, weights=dtrain.weights, base_margin=bm, ctx=ctx)
+    base0 = b.margins().copy()  # init_margin: base score or the dataset's base_margin
+    weights = np.zeros(0, np.float32)
+    arrays = None
+    info = None
+    for rnd in range(num_boost_round):
+        existing = len(weights)
+        dropped = dart_dropout(params.seed, rnd, existing, params.rate_drop, params.skip_drop)
+        if existing:
+            w = weights.copy()
+            w[dropped] = 0.0
+            m = BoostedModel.from_arrays(*arrays[:4], info[0], info[1], info[2], objective=params.objective,
+                                         weights=w, ctx=ctx)
+            d = DMatrix(dtrain.data, base_margin=None if bm is None else bm.reshape(-1), missing=dtrain.missing)
+            margins = m.predict_margin_limited(d, 0).reshape(dtrain.n_rows, k_out)
+        else:
+            margins = base0
+        b.set_margins(margins)
+        b.update(1)
+        kd = np.float32(len(dropped))
+        weights = np.concatenate([weights, np.full(k_out, np.float32(1.0) / (kd + np.float32(1.0)), np.float32)])
+        if dropped:
+            weights[dropped] = weights[dropped] * (kd / (kd + np.float32(1.0)))
+        grown = b.model()
+        arrays = grown.export()
+        info = grown.info()
+    grown = b.model()
+    off, nodes, coff, cats, _ = grown.export()
+    bs, k, f, _ = grown.info()
+    return BoostedModel.from_arrays(off, nodes, coff, cats, bs, k, f, objective=params.objective,
+                                    weights=weights, ctx=ctx)
 
 
 class EarlyStopping:
@@ -772,6 +870,11 @@ class Booster(_Native):
         out = np.zeros((self.n, self.k), np.float32)
         A.check(A.lib().sb_booster_margins(self.h, A.ptr(out, ctypes.c_float)))
         return out
+
+    def set_margins(self, margins):
+        """Replaces the margins [n][K] the next round takes its gradients from."""
+        m = np.ascontiguousarray(margins, np.float32).reshape(self.n, self.k)
+        A.check(A.lib().sb_booster_set_margins(self.h, A.ptr(m, ctypes.c_float)))
 
     def gradients(self):
         out = np.zeros((self.k, self.n, 2), np.float32)

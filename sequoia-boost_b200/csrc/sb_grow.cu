@@ -2287,6 +2287,15 @@ int sb_booster_margins(const sb_booster* b, float* out) {
   return SB_OK;
 }
 
+int sb_booster_set_margins(sb_booster* b, const float* margins) {
+  SB_REQUIRE(b && margins, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_CUDA(cudaSetDevice(b->ctx->device));
+  SB_CUDA(cudaMemcpyAsync(b->d_margin.p, margins, b->d_margin.bytes(), cudaMemcpyHostToDevice, b->ctx->stream));
+  SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+  b->delta_pending = false;  // the last tree's leaf values are not added on top
+  return SB_OK;
+}
+
 int sb_booster_gradients(const sb_booster* b, sb_gradpair* out) {
   SB_REQUIRE(b && out, SB_ERR_INVALID_ARG, "NULL argument");
   SB_CUDA(cudaMemcpyAsync(out, b->d_gpair.p, b->d_gpair.bytes(), cudaMemcpyDeviceToHost, b->ctx->stream));
