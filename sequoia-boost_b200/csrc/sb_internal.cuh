@@ -213,6 +213,10 @@ struct DevEnsemble {
   DBuf<int> tree_path;       // [n_trees + 1] first path of each tree
   DBuf<int4> shap_chunk;     // {class, first path, end path, -} work units of TreeSHAP blocks
   int n_shap_chunks = 0;
+  DBuf<int> path_fc;         // per element: its feature's index in its chunk's feature list (-1: bias)
+  DBuf<int> chunk_fo;        // [n_shap_chunks + 1] offsets into chunk_f
+  DBuf<int> chunk_f;         // the distinct features of each chunk's paths
+  int shap_max_fc = 1;       // most distinct features in one chunk
   int n_trees = 0;
   int max_depth = 0;
   int max_path_len = 0;      // elements, bias included

@@ -198,7 +198,10 @@ __global__ void k_transform(float* __restrict__ v, size_t n, int K, int objectiv
 // A block takes SHAP_ROWS rows (one per thread) over one chunk of at most
 // SHAP_CHUNK paths of one tree. Each thread adds its row's contributions
 // into a feature-major f32 partial in shared memory (its own column: no
-// conflicts, no atomics), flushed to the f64 accumulator at the end. Blocks
+// conflicts, no atomics), flushed to the f64 accumulator at the end. The
+// partial has a row only for the features the chunk's paths split on (their
+// compact indices are precomputed per element), which keeps the block's
+// shared memory small and more blocks resident. Blocks
 // stay short (a few hundred microseconds at depth 8) and have the same 128
 // threads as the margin kernels' blocks, so when a TreeSHAP block retires a
 // waiting margin block (on a higher-priority stream) fits in its place.
@@ -211,21 +214,26 @@ struct ShapPathsDev {
   const PathEl* el;
   const int* off;
   const float* leaf;
-  const int4* chunk;  // {class, first path, end path, -}
+  const int4* chunk;     // {class, first path, end path, -}
+  const int* fc;         // per element: compact feature index within its chunk
+  const int* chunk_fo;   // per chunk: offset of its feature list in chunk_f
+  const int* chunk_f;    // the chunks' distinct features
 };
 
 template <int MAXL>
 __global__ void __launch_bounds__(SHAP_ROWS) k_shap_paths(ShapPathsDev P, const float* __restrict__ X, size_t n,
                                                          int F, int K, float missing, unsigned row_blocks,
                                                          double* __restrict__ acc) {
-  extern __shared__ float ph[];          // [F][R] contributions of this block
+  extern __shared__ float ph[];          // [chunk features][R] contributions of this block
   const int R = SHAP_ROWS;
   const int tid = threadIdx.x;
   const unsigned rb = blockIdx.x % row_blocks;  // 1-D grid over (path chunk, row block)
   const size_t r0 = (size_t)rb * R;
-  const int4 ch = P.chunk[blockIdx.x / row_blocks];
+  const unsigned ci = blockIdx.x / row_blocks;
+  const int4 ch = P.chunk[ci];
   const int c = ch.x;
-  for (int i = tid; i < F * R; i += R) ph[i] = 0.0f;
+  const int fo = P.chunk_fo[ci], nfc = P.chunk_fo[ci + 1] - fo;
+  for (int i = tid; i < nfc * R; i += R) ph[i] = 0.0f;
   const float* row = X + (r0 + tid < n ? r0 + tid : r0) * (size_t)F;  // L1-resident while the block runs
   __syncwarp();
   const bool miss_nan = isnan(missing);
@@ -234,7 +242,7 @@ __global__ void __launch_bounds__(SHAP_ROWS) k_shap_paths(ShapPathsDev P, const 
       const int e0 = P.off[p], L = P.off[p + 1] - e0;
       const double leaf = (double)P.leaf[p];
       double w[MAXL], z[MAXL], iz[MAXL], o[MAXL];
-      int fe[MAXL];
+      int fe[MAXL];  // the element's row of the block's partial
 #pragma unroll
       for (int e = 0; e < MAXL; ++e) {
         fe[e] = -1;
@@ -243,7 +251,7 @@ __global__ void __launch_bounds__(SHAP_ROWS) k_shap_paths(ShapPathsDev P, const 
         o[e] = 1.0;
         if (e < L) {
           const PathEl el = P.el[e0 + e];
-          fe[e] = el.f;
+          fe[e] = P.fc[e0 + e];
           z[e] = el.z;
           iz[e] = el.inv_z;
           if (el.f >= 0) {
@@ -299,9 +307,9 @@ __global__ void __launch_bounds__(SHAP_ROWS) k_shap_paths(ShapPathsDev P, const 
   }
   if (r0 + tid < n) {
     double* a = acc + ((r0 + tid) * K + c) * (size_t)(F + 1);
-    for (int f = 0; f < F; ++f) {
-      const float v = ph[f * R + tid];
-      if (v != 0.0f) atomicAdd(a + f, (double)v);
+    for (int j = 0; j < nfc; ++j) {
+      const float v = ph[j * R + tid];
+      if (v != 0.0f) atomicAdd(a + P.chunk_f[fo + j], (double)v);
     }
   }
 }
@@ -680,6 +688,34 @@ int model_upload(sb_model* m) {
   if (!chunks.empty())
     SB_CUDA(cudaMemcpyAsync(D.shap_chunk.p, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
   D.n_shap_chunks = (int)chunks.size();
+  {  // per chunk, its paths' distinct features and each element's index among them
+    std::vector<int> pfc(pel.size(), -1), cfo(1, 0), cf, slot(std::max(m->n_features, 1), -1);
+    int maxfc = 1;
+    for (const int4& chk : chunks) {
+      const int first = (int)cf.size();
+      for (int p = chk.y; p < chk.z; ++p)
+        for (int e = poff[p]; e < poff[p + 1]; ++e) {
+          const int f = pel[e].f;
+          if (f < 0) continue;
+          if (slot[f] < 0) {
+            slot[f] = (int)cf.size() - first;
+            cf.push_back(f);
+          }
+          pfc[e] = slot[f];
+        }
+      for (size_t j = first; j < cf.size(); ++j) slot[cf[j]] = -1;
+      cfo.push_back((int)cf.size());
+      maxfc = std::max(maxfc, (int)cf.size() - first);
+    }
+    SB_TRY(D.path_fc.alloc(ctx, std::max<size_t>(pfc.size(), 1)));
+    SB_TRY(D.chunk_fo.alloc(ctx, cfo.size()));
+    SB_TRY(D.chunk_f.alloc(ctx, std::max<size_t>(cf.size(), 1)));
+    if (!pfc.empty())
+      SB_CUDA(cudaMemcpyAsync(D.path_fc.p, pfc.data(), pfc.size() * 4, cudaMemcpyHostToDevice, st));
+    SB_CUDA(cudaMemcpyAsync(D.chunk_fo.p, cfo.data(), cfo.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!cf.empty()) SB_CUDA(cudaMemcpyAsync(D.chunk_f.p, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice, st));
+    D.shap_max_fc = maxfc;
+  }
   {  // shared memory of the TreeSHAP blocks: f32 partials of SHAP_ROWS rows
     const int smem = (int)std::min<size_t>((size_t)m->n_features * SHAP_ROWS * 4, ctx->smem_optin);
     SB_TRY(raise_smem_limit((const void*)k_shap_paths<5>, (size_t)smem));
@@ -742,14 +778,18 @@ int shap_paths(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t 
   SB_CUDA(cudaMemsetAsync(d_acc, 0, n * K * (F + 1) * sizeof(double), st));
   if (T == 0 || n == 0) return SB_OK;
   const int R = SHAP_ROWS;
-  const size_t smem = (size_t)F * R * 4;
-  SB_REQUIRE(smem <= ctx->smem_optin, SB_ERR_UNSUPPORTED, "TreeSHAP on the device supports up to %zu features",
-             ctx->smem_optin / (4 * R));
+  const size_t smem = (size_t)m->dev.shap_max_fc * R * 4;
+  SB_REQUIRE(smem <= ctx->smem_optin, SB_ERR_UNSUPPORTED,
+             "TreeSHAP on the device supports up to %zu distinct features per %d paths of a tree",
+             ctx->smem_optin / (4 * R), SHAP_CHUNK);
   ShapPathsDev P;
   P.el = m->dev.path_el.p;
   P.off = m->dev.path_off.p;
   P.leaf = m->dev.path_leaf.p;
   P.chunk = m->dev.shap_chunk.p;
+  P.fc = m->dev.path_fc.p;
+  P.chunk_fo = m->dev.chunk_fo.p;
+  P.chunk_f = m->dev.chunk_f.p;
   const unsigned row_blocks = (unsigned)((n + R - 1) / R);
   SB_REQUIRE((uint64_t)row_blocks * m->dev.n_shap_chunks < (1ull << 31), SB_ERR_UNSUPPORTED,
              "TreeSHAP of %zu rows over %d path chunks exceeds one launch", n, m->dev.n_shap_chunks);
