@@ -1,7 +1,6 @@
 """The boosting loop on the GPU (sb_train / sb_booster) against the oracle's
 train_impl restatement."""
 import json
-import math
 import os
 
 import numpy as np
