@@ -53,7 +53,9 @@ def parse():
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--precision", default="fixed", choices=["fixed", "fp32"])
     ap.add_argument("--cpu-rows", type=int, default=250_000)
-    ap.add_argument("--cpu-rounds", type=int, default=3)
+    ap.add_argument("--cpu-rounds", type=int, default=20)
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-c0", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
@@ -147,6 +149,10 @@ def logloss(margin, y):
 
 
 def cpu_leg(x, y, args, sb, threads, rounds, rows):
+    """The oracle (C++ restatement of the reference CPU hist path) on the first
+    `rows` rows: binning timed apart, then one `rounds`-round training with
+    `threads` host threads. Returns (rows, seconds of the rounds, seconds of
+    binning, train logloss after the rounds)."""
     import __graft_entry__ as ge
     orc = ge._load_module("sb_pyoracle", os.path.join(ROOT, "oracle", "pyoracle.py")).Oracle()
     xs = np.ascontiguousarray(x[:rows])
@@ -155,12 +161,62 @@ def cpu_leg(x, y, args, sb, threads, rounds, rows):
     t0 = time.perf_counter()
     d = orc.data(xs, max_bin=256)
     t_bin = time.perf_counter() - t0
-    times = []
-    for _ in range(rounds):
+    t0 = time.perf_counter()
+    r = orc.train(xs, ys, p, rounds, threads=threads, data=d)
+    t_rounds = time.perf_counter() - t0
+    return xs.shape[0], t_rounds, t_bin, logloss(r["margins"].reshape(-1), ys)
+
+
+def matched_quality(sb, ctx, x, y, rows, rounds, oracle_logloss):
+    """Train logloss after the same rounds on the same row sample: the GPU's
+    fixed-point and FP32 forms against the oracle (f64 histograms of f32
+    gradients, as the reference CPU hist path)."""
+    xs = np.ascontiguousarray(x[:rows])
+    ys = np.ascontiguousarray(y[:rows])
+    d = sb.DMatrix(xs, labels=ys)
+    out = {"rows": rows, "rounds": rounds, "oracle_logloss": oracle_logloss}
+    for prec in ("fixed", "fp32"):
+        m = sb.train(params_for(sb, prec), d, rounds, ctx=ctx)
+        ll = logloss(m.predict_margin(sb.DMatrix(xs)), ys)
+        out[f"{prec}_logloss"] = ll
+        out[f"{prec}_rel_diff"] = abs(ll - oracle_logloss) / oracle_logloss
+    out["within_0.1pct"] = max(out["fixed_rel_diff"], out["fp32_rel_diff"]) < 1e-3
+    return out
+
+
+def c0_leg(sb, ctx, args):
+    """The 100k x 30 regression workload (regression_sine; reg:squarederror,
+    100 rounds, depth 6, max_bin 256, eta 0.1, lambda 1, base_score 0.5, no
+    sampling), end to end from host buffers including binning: one sb_train()
+    call on the GPU (best of 3) and the oracle on ONE host thread (as the
+    reference's README times its 1.77 s)."""
+    import __graft_entry__ as ge
+    from sequoia_boost_b200 import datagen
+    x, y = datagen.regression_sine(100_000, 30, seed=args.seed)
+    p = sb.TrainingParams(objective="reg:squarederror", max_depth=6, max_bin=256, eta=0.1, lambda_=1.0,
+                          base_score=0.5)
+    rmse = lambda pr: float(np.sqrt(np.mean((pr.astype(np.float64) - y) ** 2)))  # noqa: E731
+    sb.train(p, sb.DMatrix(x, labels=y), 100, ctx=ctx)  # warm-up
+    best = math.inf
+    for _ in range(3):
         t0 = time.perf_counter()
-        orc.train(xs, ys, p, 1, threads=threads, data=d)
-        times.append(time.perf_counter() - t0)
-    return xs.shape[0], times, t_bin
+        m = sb.train(p, sb.DMatrix(x, labels=y), 100, ctx=ctx)
+        best = min(best, time.perf_counter() - t0)
+    gpu_rmse = rmse(m.predict(sb.DMatrix(x)))
+    orc = ge._load_module("sb_pyoracle", os.path.join(ROOT, "oracle", "pyoracle.py")).Oracle()
+    p32 = sb.TrainingParams(**{**p.__dict__, "hist_precision": "fp32"})
+    t0 = time.perf_counter()
+    d = orc.data(x, max_bin=256)
+    r = orc.train(x, y, p32, 100, threads=1, data=d)
+    t_cpu = time.perf_counter() - t0
+    return {"workload": "regression_sine 100000 x 30, reg:squarederror, 100 rounds, depth 6, max_bin 256, "
+                        "eta 0.1, lambda 1, base_score 0.5",
+            "gpu_e2e_s": best, "gpu_mrow_rounds_per_s": 100_000 * 100 / best / 1e6, "gpu_train_rmse": gpu_rmse,
+            "oracle_1thread_s": t_cpu, "oracle_mrow_rounds_per_s": 100_000 * 100 / t_cpu / 1e6,
+            "oracle_train_rmse": rmse(r["margins"].reshape(-1)),
+            "speedup_e2e": t_cpu / best,
+            "reference_readme": "1.77 s on 1 thread (README.md:117-125), U(0,1) polynomial data of the same "
+                                "shape; this oracle time calibrates the port against it"}
 
 
 def _pct(v, q):
@@ -409,10 +465,35 @@ def main():
                 "bytes_per_launch": st["hist_bytes"] / max(st["hist_launches"], 1),
                 "ms_per_launch": st["hist_ms"] / max(st["hist_launches"], 1),
                 "hist_share_of_round": st["hist_ms"] / st["round_ms"] if st["round_ms"] else None}
-    quality = {"train_logloss_after_rounds": logloss(b.margins().reshape(-1), y),
-               "rounds": args.warmup + args.steps + min(args.steps, 5),
+    rounds_total = args.warmup + args.steps + min(args.steps, 5)
+    quality = {"train_logloss_fixed": logloss(b.margins().reshape(-1), y), "rounds": rounds_total,
                "quant_err_grad": st["quant_err_grad"], "quant_err_hess": st["quant_err_hess"]}
     del b
+
+    fp32 = None
+    if args.precision == "fixed" and not args.no_fp32:
+        # the plain FP32 histogram form on the same resident index, same rounds
+        b32 = sb.Booster(gh, params_for(sb, "fp32"), y, ctx=ctx)
+        for _ in range(args.warmup):
+            b32.update(1)
+        ctx.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            b32.update(1)
+        e1.record(stream)
+        ctx.synchronize()
+        ms32 = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+        b32.set_timing(True)
+        b32.reset_stats()
+        b32.update(min(args.steps, 5))
+        st32 = b32.stats()
+        quality["train_logloss_fp32"] = logloss(b32.margins().reshape(-1), y)
+        quality["fixed_vs_fp32_rel_diff"] = (abs(quality["train_logloss_fixed"] - quality["train_logloss_fp32"])
+                                             / quality["train_logloss_fp32"])
+        fp32 = {"value": job_value(world, n, args.steps, ms32), "unit": UNIT, "ms_per_step": ms32 / args.steps,
+                "hist_ms_per_launch": st32["hist_ms"] / max(st32["hist_launches"], 1),
+                "fixed_over_fp32": value / job_value(world, n, args.steps, ms32)}
+        del b32
     del gh
 
     e2e = None
@@ -435,13 +516,18 @@ def main():
         del m, xp, yp
 
     cpu = None
+    matched = None
+    c0 = None
     if not args.no_cpu and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        rows, times, t_bin = cpu_leg(x, y, args, sb, threads, args.cpu_rounds, args.cpu_rows)
-        cpu = {"value": rows * len(times) / sum(times) / 1e6, "unit": UNIT, "cores": threads,
+        rows, t_rounds, t_bin, orc_ll = cpu_leg(x, y, args, sb, threads, args.cpu_rounds, args.cpu_rows)
+        cpu = {"value": rows * args.cpu_rounds / t_rounds / 1e6, "unit": UNIT, "cores": threads,
                "kind": "port",
-               "sample": f"first {rows} rows, {len(times)} rounds, binning excluded "
+               "sample": f"first {rows} rows, one {args.cpu_rounds}-round training, binning excluded "
                          f"(binning {t_bin:.1f} s single-threaded)"}
+        matched = matched_quality(sb, ctx, x, y, rows, args.cpu_rounds, orc_ll)
+        if not args.no_c0:
+            c0 = c0_leg(sb, ctx, args)
     serving = None
     if not args.no_serve and rank == 0:
         serving = serving_leg(sb, ctx, args, torch)
@@ -452,7 +538,7 @@ def main():
                 "dtype": "i64" if args.precision == "fixed" else "f32", "data": "synthetic",
                 "config": config_of(args, n), "clocks": clk, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "quality": quality,
-                "serving": serving}
+                "fp32_arm": fp32, "matched_quality": matched, "c0": c0, "serving": serving}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -85,6 +85,12 @@ enum { /* create_objective, objective/mod.rs:136-161 */
 
 enum { SB_GROW_DEPTHWISE = 0, SB_GROW_LOSSGUIDE = 1 }; /* config GrowPolicy */
 
+enum { /* config TreeMethod (params.rs); Auto resolves to hist (train.rs:60-64) */
+  SB_TREE_HIST = 0,   /* cuts and bins computed once */
+  SB_TREE_APPROX = 1  /* hessian-weighted cuts recomputed every round and class
+                         (train.rs:46-53); trains through sb_train only */
+};
+
 enum { /* histogram accumulation on the device */
   SB_HIST_FP32 = 0,  /* f32 shared-memory partials, f64 node histograms */
   SB_HIST_FIXED = 1  /* per-round power-of-two int quantised gradients,
@@ -117,11 +123,11 @@ typedef struct sb_train_params {
   int32_t max_leaves;         /* 0 */
   int32_t grow_policy;        /* SB_GROW_* */
   int32_t max_bin;            /* 256 */
-  int32_t hist_precision;     /* SB_HIST_* */
+  int32_t hist_precision;     /* SB_HIST_*, default SB_HIST_FIXED (deterministic) */
   int32_t quantize_bits;      /* fixed-point magnitude bits, 0 = 16 */
   int32_t n_monotone;
   int32_t n_interaction_groups;
-  int32_t reserved;
+  int32_t tree_method;        /* SB_TREE_*, default SB_TREE_HIST */
 } sb_train_params;
 
 /* Fills `p` with the reference defaults (params.rs:153-186). */
@@ -186,6 +192,14 @@ int sb_ghist_cuts(const sb_ghist* g, uint32_t* feature_offset, float* cut_values
  * reference's global bin is feature_offset[f] + local (ghist.rs:48-82). */
 int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins);
 
+/* HistCuts::from_dmatrix_weighted (data/quantile.rs:81-122, with
+ * build_feature_cuts_weighted :253-316) + GHistIndex::from_dmatrix: the cuts
+ * and bins tree_method=approx uses in a round, numeric cuts placed at the
+ * hessian-weighted quantiles of `hessians` (one per row, finite, >= 0; host). */
+int sb_ghist_create_weighted(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
+                             const uint8_t* feature_types, float missing, int max_bin, const float* hessians,
+                             sb_ghist** out);
+
 /* -------------------------------------------- HistogramBackend (the seam)
  * trait HistogramBackend::build, tree/hist/mod.rs:31-45 / CpuBackend::build
  * :58-89: out[bin] = sum over rows r and r's bins of (grad_r, hess_r), f64,
@@ -206,7 +220,10 @@ int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats
  * the caller's DEVICE buffers: d_rows[m] (row ids below n), d_gpair[n] and
  * d_out[total_bins] (overwritten), on the context's device.
  * Working memory is one static device array of SB_STATIC_SCRATCH_BYTES
- * (8 MiB). The node histogram in it takes 16 bytes per bin plus one missing
+ * (8 MiB). It is part of the library's device code, so every device on which
+ * the library's kernels are loaded holds those 8 MiB until the process exits,
+ * whether or not this entry point is ever called. The `g` index must have been
+ * built on the context's device. The node histogram in it takes 16 bytes per bin plus one missing
  * bin per feature, so total_bins + n_cols must stay below about 524,000;
  * a larger index is rejected with SB_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's address
@@ -219,6 +236,18 @@ int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats
 int sb_hist_build_static(sb_ctx* ctx, const sb_ghist* g, const uint32_t* d_rows, size_t m,
                          const sb_gradpair* d_gpair, size_t n, sb_gradstats* d_out,
                          size_t total_bins);
+
+/* ------------------------------------------------------------ objectives
+ * Objective::gradient, objective/mod.rs:58-69, for the objectives of the hist
+ * path: squared error and pseudo-Huber (objective/regression.rs:18-85),
+ * logistic with scale_pos_weight (classification.rs:50-71) and softmax
+ * (multiclass.rs:64-91). `preds` are margins [n_rows][K] (K = num_class for
+ * the multiclass objectives, else 1), `labels` [n_rows], `weights` [n_rows] or
+ * NULL; `out` receives GradPair [n_rows][K]. Host buffers. Computed by the
+ * same device code as the boosting rounds' gradients. */
+int sb_objective_gradient(sb_ctx* ctx, int objective, int num_class, double scale_pos_weight,
+                          const float* preds, const float* labels, const float* weights, size_t n_rows,
+                          sb_gradpair* out);
 
 /* ---------------------------------------------------- tree / boosting loop */
 typedef struct sb_model sb_model;

@@ -46,7 +46,7 @@ class Params(ctypes.Structure):
                 ("max_leaves", ctypes.c_int32), ("grow_policy", ctypes.c_int32),
                 ("max_bin", ctypes.c_int32), ("hist_precision", ctypes.c_int32),
                 ("quantize_bits", ctypes.c_int32), ("n_monotone", ctypes.c_int32),
-                ("n_interaction_groups", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("n_interaction_groups", ctypes.c_int32), ("tree_method", ctypes.c_int32)]
 
 
 class ModelView(ctypes.Structure):
@@ -75,6 +75,7 @@ U8P = ctypes.POINTER(ctypes.c_uint8)
 I64P = ctypes.POINTER(ctypes.c_int64)
 SIGS = {
     "orc_data_create": (P, [FP, SZ, SZ, U8P, ctypes.c_float, ctypes.c_int]),
+    "orc_data_create_weighted": (P, [FP, SZ, SZ, U8P, ctypes.c_float, ctypes.c_int, FP]),
     "orc_data_destroy": (None, [P]),
     "orc_data_total_bins": (SZ, [P]),
     "orc_data_is_dense": (ctypes.c_int, [P]),
@@ -87,6 +88,8 @@ SIGS = {
                            ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int]),
     "orc_train": (P, [P, FP, ctypes.POINTER(Params), FP, FP, FP, ctypes.c_int, ctypes.c_int, FP,
                       ctypes.POINTER(ctypes.c_double)]),
+    "orc_train_dart": (P, [P, FP, ctypes.POINTER(Params), ctypes.c_double, ctypes.c_double, FP, FP, FP,
+                           ctypes.c_int, ctypes.c_int, FP]),
     "orc_model_destroy": (None, [P]),
     "orc_model_sizes": (None, [P, ctypes.POINTER(ctypes.c_int32), I64P, I64P]),
     "orc_model_export": (None, [P, I64P, ctypes.POINTER(Node), I64P, U32P, FP, FP]),
@@ -137,6 +140,7 @@ def make_params(tp):
     p.grow_policy = 1 if tp.grow_policy == "lossguide" else 0
     p.max_bin = tp.max_bin
     p.hist_precision = 1 if tp.hist_precision == "fixed" else 0
+    p.tree_method = 1 if getattr(tp, "tree_method", "hist") == "approx" else 0
     p.quantize_bits = tp.quantize_bits
     keep = []
     if tp.monotone_constraints:
@@ -179,6 +183,18 @@ class Oracle:
     def cuts(self, x, ftypes=None, missing=float("nan"), max_bin=256):
         return self.data(x, ftypes, missing, max_bin).cuts()
 
+    def data_weighted(self, x, hessians, ftypes=None, missing=float("nan"), max_bin=256):
+        """HistCuts::from_dmatrix_weighted (tree_method=approx) + GHistIndex."""
+        x = np.ascontiguousarray(x, np.float32)
+        w = np.ascontiguousarray(hessians, np.float32)
+        assert w.size == x.shape[0]
+        ft = None if ftypes is None else np.ascontiguousarray(ftypes, np.uint8)
+        h = self.lib.orc_data_create_weighted(_p(x, ctypes.c_float), x.shape[0], x.shape[1],
+                                              _p(ft, ctypes.c_uint8), missing, max_bin, _p(w, ctypes.c_float))
+        if not h:
+            raise ValueError("oracle rejected the dataset")
+        return OData(self, h, x.shape[0], x.shape[1])
+
     # ---- trees / training
     def tree_build(self, d, params, gpair, rows, round_=0, k=0, threads=1):
         p, keep = make_params(params)
@@ -206,6 +222,25 @@ class Oracle:
             raise ValueError("oracle rejected the parameters")
         return {"model": OModel(self, h), "margins": margins,
                 "metric": None if metric is None else metric[:rounds]}
+
+    def train_dart(self, x, y, params, rounds, weights=None, base_margin=None, ftypes=None,
+                   missing=float("nan"), threads=1):
+        """dart_round (learner/train.rs:384-456); the model's export holds the
+        tree weights."""
+        d = self.data(x, ftypes, missing, params.max_bin)
+        p, keep = make_params(params)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        bm = None if base_margin is None else np.ascontiguousarray(base_margin, np.float32)
+        k = params.num_class if params.objective.startswith("multi:") else 1
+        margins = np.zeros((x.shape[0], k), np.float32)
+        h = self.lib.orc_train_dart(d.h, _p(x, ctypes.c_float), ctypes.byref(p), float(params.rate_drop),
+                                    float(params.skip_drop), _p(y, ctypes.c_float), _p(w, ctypes.c_float),
+                                    _p(bm, ctypes.c_float), rounds, threads, _p(margins, ctypes.c_float))
+        if not h:
+            raise ValueError("oracle rejected the parameters")
+        return {"model": OModel(self, h), "margins": margins}
 
     def sample_features(self, F, params, round_=0, k=0, nid=0):
         p, keep = make_params(params)

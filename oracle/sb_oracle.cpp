@@ -282,6 +282,49 @@ void build_feature_cuts(const std::vector<float>& sv, size_t max_bin, std::vecto
   push_max_sentinel(out, max_val);
 }
 
+// Hessian-weighted cuts of tree_method=approx, quantile.rs:253-316: `sv`
+// holds ascending (value, weight) pairs (a stable sort by value keeps row
+// order among equal values).
+void build_feature_cuts_weighted(const std::vector<std::pair<float, float>>& sv, size_t max_bin,
+                                 std::vector<float>& out) {
+  if (sv.empty()) { out.push_back(0.0f); return; }
+  const float max_val = sv.back().first;
+  size_t distinct = 1;
+  for (size_t i = 1; i < sv.size(); ++i)
+    if (sv[i - 1].first != sv[i].first) distinct++;
+  if (distinct <= max_bin) {  // every distinct value is a cut; weights do not matter
+    out.push_back(sv[0].first);
+    for (size_t i = 1; i < sv.size(); ++i)
+      if (sv[i - 1].first != sv[i].first) out.push_back(sv[i].first);
+  } else {
+    double total = 0.0;  // the sequential f64 sum of the weights in value order
+    for (const auto& p : sv) total += (double)p.second;
+    float last = -INFINITY;
+    if (total > 0.0) {
+      const double step = total / (double)max_bin;
+      double cum = 0.0;
+      size_t b = 1;
+      for (const auto& p : sv) {
+        cum += (double)p.second;
+        while (b <= max_bin && cum + 1e-12 >= (double)b * step) {
+          if (p.first > last) { out.push_back(p.first); last = p.first; }
+          b++;
+        }
+      }
+    } else {  // all weights zero: the unweighted positions
+      const size_t n = sv.size();
+      for (size_t b = 1; b <= max_bin; ++b) {
+        const double q = (double)b / (double)max_bin;
+        const size_t c = (size_t)std::ceil(q * (double)n);
+        const size_t idx = std::min(std::max(c, (size_t)1) - 1, n - 1);
+        const float v = sv[idx].first;
+        if (v > last) { out.push_back(v); last = v; }
+      }
+    }
+  }
+  push_max_sentinel(out, max_val);
+}
+
 // ---------------------------------------------------------------- ghist
 }  // namespace
 
@@ -987,8 +1030,19 @@ int scale_exp(float m, int bits) {
 // =================================================================== C ABI
 extern "C" {
 
+// HistCuts::from_dmatrix (quantile.rs:39-70) or, with `hessians` (one per
+// row), HistCuts::from_dmatrix_weighted (quantile.rs:81-122), then
+// GHistIndex::from_dmatrix.
+orc_data* orc_data_create_weighted(const float* X, size_t n, size_t F, const uint8_t* ftypes, float missing,
+                                   int max_bin, const float* hessians);
+
 orc_data* orc_data_create(const float* X, size_t n, size_t F, const uint8_t* ftypes, float missing,
                           int max_bin) {
+  return orc_data_create_weighted(X, n, F, ftypes, missing, max_bin, nullptr);
+}
+
+orc_data* orc_data_create_weighted(const float* X, size_t n, size_t F, const uint8_t* ftypes, float missing,
+                                   int max_bin, const float* hessians) {
   if (!X || n == 0 || F == 0 || max_bin < 2) return nullptr;
   if (!std::isnan(missing))
     for (size_t i = 0; i < n * F; ++i)
@@ -1002,16 +1056,26 @@ orc_data* orc_data_create(const float* X, size_t n, size_t F, const uint8_t* fty
   c.off.push_back(0);
   c.is_cat.assign(F, 0);
   std::vector<float> col;
+  std::vector<std::pair<float, float>> wcol;
   for (size_t f = 0; f < F; ++f) {  // from_dmatrix, quantile.rs:39-70 (to_csc order)
     col.clear();
+    wcol.clear();
     for (size_t r = 0; r < n; ++r) {
       float v = X[r * F + f];
-      if (!is_missing(v, missing)) col.push_back(v);
+      if (is_missing(v, missing)) continue;
+      col.push_back(v);
+      if (hessians) wcol.emplace_back(v, hessians[r]);
     }
     std::stable_sort(col.begin(), col.end(), [](float a, float b) { return a < b; });
     if (ftypes && ftypes[f] == SB_FEAT_CATEGORICAL) {
       c.is_cat[f] = 1;
       build_categorical_cuts(col, c.vals);
+    } else if (hessians) {  // from_dmatrix_weighted, quantile.rs:103-114
+      std::stable_sort(wcol.begin(), wcol.end(),
+                       [](const std::pair<float, float>& a, const std::pair<float, float>& b) {
+                         return a.first < b.first;
+                       });
+      build_feature_cuts_weighted(wcol, (size_t)max_bin, c.vals);
     } else {
       build_feature_cuts(col, (size_t)max_bin, c.vals);
     }
@@ -1152,10 +1216,11 @@ void orc_gradient(int objective, int num_class, double spw, const float* preds, 
         std::memcpy(probs.data(), preds + i * k, k * sizeof(float));
         softmax_inplace(probs.data(), k);
         float w = weights ? weights[i] : 1.0f;
-        size_t label = (size_t)labels[i];
+        // `labels[i] as usize` saturates: negative and NaN labels are class 0
+        const uint32_t label = f32_as_u32(labels[i]);
         for (int c = 0; c < k; ++c) {
           float p = probs[c];
-          float target = ((size_t)c == label) ? 1.0f : 0.0f;
+          float target = ((uint32_t)c == label) ? 1.0f : 0.0f;
           float grad = (p - target) * w;
           float hess = std::max(2.0f * p * (1.0f - p) * w, 1e-16f);
           out[i * k + c] = sb_gradpair{grad, hess};
@@ -1264,9 +1329,21 @@ orc_model* orc_train(const orc_data* d, const float* X, const sb_train_params* p
     }
     for (int k = 0; k < K; ++k) {
       for (size_t r = 0; r < n; ++r) gk[r] = gpair[r * K + k];
+      const orc_data* dk = d;
+      std::unique_ptr<orc_data> dw;
+      if (p->tree_method == SB_TREE_APPROX) {  // Prepared::Approx, train.rs:46-53
+        std::vector<float> hess(n);
+        for (size_t r = 0; r < n; ++r) hess[r] = gk[r].hess;
+        dw.reset(orc_data_create_weighted(X, n, F, d->cuts.is_cat.data(), d->missing, p->max_bin, hess.data()));
+        if (!dw) {
+          delete mdl;
+          return nullptr;
+        }
+        dk = dw.get();
+      }
       if (p->hist_precision == SB_HIST_FIXED) orc_quantize(gk.data(), n, bits, gk.data(), nullptr, nullptr);
       Sampler s = make_sampler(F, *p, (uint64_t)round, (uint64_t)k);
-      OTree t = builder.build(*d, gk.data(), rows.data(), rows.size(), s, threads);
+      OTree t = builder.build(*dk, gk.data(), rows.data(), rows.size(), s, threads);
       float eta = (float)p->eta;
       for (auto& nd : t.nodes)  // scale_leaves, regtree.rs:201-207
         if (nd.left == -1) nd.leaf_value *= eta;
@@ -1283,6 +1360,92 @@ orc_model* orc_train(const orc_data* d, const float* X, const sb_train_params* p
     }
   }
   if (margins_out) std::memcpy(margins_out, margin.data(), n * K * sizeof(float));
+  return mdl;
+}
+
+// dart_round (learner/train.rs:384-456) with the dropout draws taken from the
+// SplitMix64 stream keyed by sb_dart_key (the reference's rand 0.8 StdRng is
+// not available); row and column sampling use the hist path's keys. Tree
+// weights come back in weights_out (one per tree, n_trees = rounds * K).
+orc_model* orc_train_dart(const orc_data* d, const float* X, const sb_train_params* p, double rate_drop,
+                          double skip_drop, const float* labels, const float* weights, const float* base_margin,
+                          int rounds, int threads, float* margins_out) {
+  if (orc_validate(p) != 0 || !labels) return nullptr;
+  const size_t n = d->n, F = d->F;
+  const int K = n_outputs(p->objective, p->num_class);
+  const float base = orc_base_margin(p, labels, weights, n);
+  orc_model* mdl = new orc_model;
+  mdl->base_score = base;
+  mdl->num_class = p->num_class;
+  mdl->n_features = (int)F;
+  mdl->objective = p->objective;
+  const std::vector<float> init = init_margin(base_margin, base_margin ? n : 0, n, K, base);
+  std::vector<sb_gradpair> gpair(n * K), gk(n);
+  std::vector<uint32_t> rows;
+  std::vector<float> margin(n * K);
+  Builder builder(*p, F);
+  const int bits = p->quantize_bits > 0 ? p->quantize_bits : 16;
+  for (int round = 0; round < rounds; ++round) {
+    // 1. the dropout set (train.rs:397-425)
+    const size_t existing = mdl->trees.size();
+    std::vector<size_t> drop;
+    sb_splitmix g{sb_dart_key(p->seed, (uint64_t)round)};
+    const bool skip = sb_u01(sb_splitmix_next(&g)) < skip_drop;
+    if (!skip && existing > 0) {
+      for (size_t i = 0; i < existing; ++i)
+        if (sb_u01(sb_splitmix_next(&g)) < rate_drop) drop.push_back(i);
+      if (drop.empty()) drop.push_back((size_t)sb_splitmix_bounded(&g, existing));
+    }
+    // 2. the ensemble's margins without the dropout set (model.rs:130-145)
+    std::vector<uint8_t> dropped(existing, 0);
+    for (size_t i : drop) dropped[i] = 1;
+    margin = init;
+    for (size_t t = 0; t < existing; ++t) {
+      if (dropped[t]) continue;
+      const float w = mdl->weights[t];
+      const size_t cls = t % K;
+      for (size_t r = 0; r < n; ++r)
+        margin[r * K + cls] += w * mdl->trees[t].nodes[leaf_id(mdl->trees[t], X + r * F, d->missing)].leaf_value;
+    }
+    orc_gradient(p->objective, p->num_class, p->scale_pos_weight, margin.data(), labels, weights, n,
+                 gpair.data());
+    // 3. one new tree per output, weight 1 / (k + 1)
+    rows.clear();
+    if (p->subsample >= 1.0) {
+      for (size_t r = 0; r < n; ++r) rows.push_back((uint32_t)r);
+    } else {
+      const uint64_t rk = sb_round_key(p->seed, (uint64_t)round);
+      for (size_t r = 0; r < n; ++r)
+        if (sb_u01(sb_row_draw(rk, r)) < p->subsample) rows.push_back((uint32_t)r);
+      if (rows.empty()) rows.push_back((uint32_t)sb_row_fallback(rk, n));
+    }
+    const float kd = (float)drop.size();
+    const float new_weight = 1.0f / (kd + 1.0f);
+    for (int k = 0; k < K; ++k) {
+      for (size_t r = 0; r < n; ++r) gk[r] = gpair[r * K + k];
+      if (p->hist_precision == SB_HIST_FIXED) orc_quantize(gk.data(), n, bits, gk.data(), nullptr, nullptr);
+      Sampler smp = make_sampler(F, *p, (uint64_t)round, (uint64_t)k);
+      OTree t = builder.build(*d, gk.data(), rows.data(), rows.size(), smp, threads);
+      const float eta = (float)p->eta;
+      for (auto& nd : t.nodes)  // scale_leaves, regtree.rs:201-207
+        if (nd.left == -1) nd.leaf_value *= eta;
+      mdl->trees.push_back(std::move(t));
+      mdl->weights.push_back(new_weight);
+    }
+    // 4. the dropped trees scaled by k / (k + 1)
+    const float factor = kd / (kd + 1.0f);
+    for (size_t i : drop) mdl->weights[i] *= factor;
+  }
+  if (margins_out) {  // the final model's margins with its tree weights
+    margin = init;
+    for (size_t t = 0; t < mdl->trees.size(); ++t) {
+      const float w = mdl->weights[t];
+      const size_t cls = t % K;
+      for (size_t r = 0; r < n; ++r)
+        margin[r * K + cls] += w * mdl->trees[t].nodes[leaf_id(mdl->trees[t], X + r * F, d->missing)].leaf_value;
+    }
+    std::memcpy(margins_out, margin.data(), n * K * sizeof(float));
+  }
   return mdl;
 }
 

@@ -36,6 +36,10 @@ typedef struct orc_model orc_model;
  * sort would panic). */
 orc_data* orc_data_create(const float* X, size_t n, size_t F, const uint8_t* ftypes,
                           float missing, int max_bin);
+/* HistCuts::from_dmatrix_weighted (data/quantile.rs:81-122, cuts of
+ * tree_method=approx, weighted by one hessian per row) + GHistIndex. */
+orc_data* orc_data_create_weighted(const float* X, size_t n, size_t F, const uint8_t* ftypes, float missing,
+                                   int max_bin, const float* hessians);
 void orc_data_destroy(orc_data* d);
 size_t orc_data_total_bins(const orc_data* d);
 int orc_data_is_dense(const orc_data* d);
@@ -62,6 +66,11 @@ orc_model* orc_tree_build(const orc_data* d, const sb_train_params* p,
 orc_model* orc_train(const orc_data* d, const float* X, const sb_train_params* p,
                      const float* labels, const float* weights, const float* base_margin,
                      int rounds, int threads, float* margins_out, double* metric_out);
+/* dart_round (learner/train.rs:384-456): DART training with the dropout
+ * draws of sb_dart_key's stream; tree weights via orc_model_export. */
+orc_model* orc_train_dart(const orc_data* d, const float* X, const sb_train_params* p, double rate_drop,
+                          double skip_drop, const float* labels, const float* weights, const float* base_margin,
+                          int rounds, int threads, float* margins_out);
 
 void orc_model_destroy(orc_model* m);
 void orc_model_sizes(const orc_model* m, int32_t* n_trees, int64_t* n_nodes, int64_t* n_cats);

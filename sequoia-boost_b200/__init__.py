@@ -13,6 +13,7 @@ src/lib.rs:86-97) over the C ABI in include/sb_gpu.h:
     GpuBackend       tree/hist/mod.rs:31-45 (HistogramBackend: build, subtract)
     HistTreeBuilder  tree/builder/hist.rs:98-202
     Booster          the device-resident state of train_impl's round loop
+    objective_gradient  objective/mod.rs:58-69 (Objective::gradient)
 
 All compute runs in libsb_gpu.so on an sm_100 GPU; there is no CPU fallback.
 """
@@ -26,6 +27,7 @@ from .api import (  # noqa: F401
     HistTreeBuilder,
     Monotone,
     Server,
+    objective_gradient,
     TrainingParams,
     default_context,
     train,
@@ -36,6 +38,6 @@ from ._abi import SbError  # noqa: F401
 
 __all__ = [
     "BoostedModel", "Booster", "Context", "DMatrix", "GHistIndex", "GpuBackend",
-    "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "train", "train_many",
+    "HistTreeBuilder", "Monotone", "SbError", "Server", "TrainingParams", "default_context", "objective_gradient", "train", "train_many",
     "train_with_eval",
 ]

@@ -32,6 +32,8 @@ SB_GROW_DEPTHWISE = 0
 SB_GROW_LOSSGUIDE = 1
 SB_HIST_FP32 = 0
 SB_HIST_FIXED = 1
+SB_TREE_HIST = 0
+SB_TREE_APPROX = 1
 
 
 class SbGradPair(ctypes.Structure):
@@ -88,7 +90,7 @@ class SbTrainParams(ctypes.Structure):
         ("quantize_bits", ctypes.c_int32),
         ("n_monotone", ctypes.c_int32),
         ("n_interaction_groups", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("tree_method", ctypes.c_int32),
     ]
 
 
@@ -180,6 +182,9 @@ SIGNATURES = {
     "sb_hist_subtract": (I32, [P, ctypes.POINTER(SbGradStats), ctypes.POINTER(SbGradStats),
                                ctypes.POINTER(SbGradStats), SZ]),
     "sb_hist_build_static": (I32, [P, P, P, SZ, P, SZ, P, SZ]),  # device pointers
+    "sb_objective_gradient": (I32, [P, I32, I32, ctypes.c_double, F32P, F32P, F32P, SZ,
+                                    ctypes.POINTER(SbGradPair)]),
+    "sb_ghist_create_weighted": (I32, [P, F32P, SZ, SZ, U8P, ctypes.c_float, I32, F32P, ctypes.POINTER(P)]),
     "sb_tree_build": (I32, [P, P, ctypes.POINTER(SbTrainParams), ctypes.POINTER(SbGradPair), SZ,
                             U32P, SZ, ctypes.c_uint64, ctypes.c_uint32, I32P, ctypes.POINTER(P)]),
     "sb_booster_create": (I32, [P, P, ctypes.POINTER(SbTrainParams), F32P, F32P, F32P,

@@ -30,8 +30,13 @@ class Monotone:
 @dataclass
 class TrainingParams:
     """TrainingParams with the reference's field names and defaults
-    (config/params.rs:76-186). `hist_precision` ("fp32" | "fixed") and
-    `quantize_bits` select this backend's histogram form."""
+    (config/params.rs:76-186). `hist_precision` ("fixed" | "fp32") and
+    `quantize_bits` select this backend's histogram form. The default is the
+    fixed-point form: each round's gradient pairs are rounded to integers with
+    a power-of-two scale and summed exactly in int64, so two trainings with the
+    same data, parameters and seed give identical models, as the reference's
+    do (tests/properties.rs:40-46). "fp32" sums f32 gradients with atomics
+    whose order varies from run to run."""
     seed: int = 0
     objective: str = "reg:squarederror"
     num_class: int = 0
@@ -50,10 +55,11 @@ class TrainingParams:
     alpha: float = 0.0
     scale_pos_weight: float = 1.0
     grow_policy: str = "depthwise"
+    tree_method: str = "hist"  # "auto" | "hist" | "approx" (params.rs TreeMethod; "exact" is not built)
     max_bin: int = 256
     monotone_constraints: List[int] = field(default_factory=list)
     interaction_constraints: List[List[int]] = field(default_factory=list)
-    hist_precision: str = "fp32"
+    hist_precision: str = "fixed"
     quantize_bits: int = 0
     eval_metric: List[str] = field(default_factory=list)  # XGBoost `eval_metric` (params.rs:96-97)
     booster: str = "gbtree"  # "gbtree" | "dart" (params.rs:79; gblinear is not built)
@@ -89,6 +95,10 @@ class TrainingParams:
         p.alpha = self.alpha
         p.scale_pos_weight = self.scale_pos_weight
         p.grow_policy = A.SB_GROW_LOSSGUIDE if self.grow_policy == "lossguide" else A.SB_GROW_DEPTHWISE
+        if self.tree_method not in ("auto", "hist", "approx"):
+            code = A.SB_ERR_UNSUPPORTED if self.tree_method == "exact" else A.SB_ERR_INVALID_ARG
+            raise A.SbError(code, f"tree_method `{self.tree_method}` is not available (auto, hist, approx)")
+        p.tree_method = A.SB_TREE_APPROX if self.tree_method == "approx" else A.SB_TREE_HIST
         p.max_bin = self.max_bin
         p.hist_precision = A.SB_HIST_FIXED if self.hist_precision == "fixed" else A.SB_HIST_FP32
         p.quantize_bits = self.quantize_bits
@@ -297,6 +307,24 @@ class GHistIndex(_Native):
         A.check(A.lib().sb_ghist_create_device(self.ctx.h, ctypes.c_void_p(d_ptr), n_rows, n_cols,
                                                A.ptr(ft, ctypes.c_uint8), missing, max_bin,
                                                ctypes.byref(h)))
+        self.h = h
+        self._adopt(self.ctx)
+        self._keep = ft
+        return self
+
+    @classmethod
+    def weighted(cls, dmat: DMatrix, hessians, max_bin=256, ctx: Context = None):
+        """HistCuts::from_dmatrix_weighted + GHistIndex::from_dmatrix
+        (data/quantile.rs:81-122): the cuts and bins of one tree_method=approx
+        round, numeric cuts at the hessian-weighted quantiles."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        ft = dmat._ftypes()
+        hs = _f32(hessians).reshape(-1)
+        h = ctypes.c_void_p()
+        A.check(A.lib().sb_ghist_create_weighted(self.ctx.h, A.ptr(dmat.data, ctypes.c_float), dmat.n_rows,
+                                                 dmat.n_cols, A.ptr(ft, ctypes.c_uint8), dmat.missing, max_bin,
+                                                 A.ptr(hs, ctypes.c_float), ctypes.byref(h)))
         self.h = h
         self._adopt(self.ctx)
         self._keep = ft
@@ -565,6 +593,25 @@ class BoostedModel(_Native):
 
     def _free(self, _A=A):
         _A.lib().sb_model_destroy(self.h)
+
+
+def objective_gradient(objective, preds, labels, weights=None, num_class=0, scale_pos_weight=1.0,
+                       ctx: Context = None):
+    """Objective::gradient (objective/mod.rs:58-69) on the device: margins
+    `preds` [n][K] -> GradPair [n][K] as an (n*K, 2) f32 array, with the code
+    the boosting rounds use (sb_objective_gradient)."""
+    ctx = ctx or default_context()
+    if objective not in OBJECTIVES:
+        raise A.SbError(A.SB_ERR_INVALID_ARG, f"unknown value `{objective}` for objective")
+    preds = _f32(preds).reshape(-1)
+    labels = _f32(labels).reshape(-1)
+    w = None if weights is None else _f32(weights).reshape(-1)
+    out = np.zeros((preds.size, 2), np.float32)
+    A.check(A.lib().sb_objective_gradient(ctx.h, OBJECTIVES[objective], num_class, float(scale_pos_weight),
+                                          A.ptr(preds, ctypes.c_float), A.ptr(labels, ctypes.c_float),
+                                          A.ptr(w, ctypes.c_float), labels.size,
+                                          out.ctypes.data_as(ctypes.POINTER(A.SbGradPair))))
+    return out
 
 
 def train(params: TrainingParams, dtrain: DMatrix, num_boost_round: int, ctx: Context = None):

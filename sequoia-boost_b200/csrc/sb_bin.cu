@@ -363,51 +363,51 @@ __global__ void __launch_bounds__(1024) k_cuts_plan(
   }
 }
 
-// K2: local bin of every entry; categorical exact match (unseen -> 0).
-__global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t n, int F, int Fp,
+// K2: local bin of every entry; categorical exact match (unseen -> 0). The
+// histogram codes go to row r at position rpos[f] (rbase[f] + local bin, or
+// rmiss[f] when missing); the feature-major copy holds the local bin itself,
+// MISSING_BIN when missing.
+__global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t n, int F, size_t Fp,
                                              float missing, const uint32_t* __restrict__ foff,
                                              const float* __restrict__ cuts,
                                              const uint8_t* __restrict__ is_cat,
-                                             const int* __restrict__ fbase,
-                                             const int* __restrict__ fmiss,
+                                             const int* __restrict__ rpos,
+                                             const int* __restrict__ rbase,
+                                             const int* __restrict__ rmiss,
                                              uint16_t* __restrict__ bins,
                                              uint16_t* __restrict__ bins_col) {
   const bool miss_nan = isnan(missing);
-  size_t total = n * (size_t)Fp;
+  const size_t total = n * (size_t)F;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
-    size_t r = i / Fp;
-    int f = (int)(i - r * Fp);
-    uint16_t out = MISSING_BIN;  // padding columns
-    if (f < F) {
-      float v = X[r * F + f];
-      out = (uint16_t)fmiss[f];
-      if (!is_missing_d(v, missing, miss_nan)) {
-        uint32_t s = foff[f], e = foff[f + 1];
-        uint32_t len = e - s;
-        if (is_cat[f]) {
-          uint32_t lo = 0, hi = len, found = 0;
-          while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            float c = cuts[s + mid];
-            if (c < v) lo = mid + 1;
-            else if (c > v) hi = mid;
-            else { found = mid; break; }
-          }
-          out = (uint16_t)(fbase[f] + (int)found);
-        } else {
-          uint32_t lo = 0, hi = len;  // partition_point(c <= v)
-          while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
-          }
-          uint32_t local = lo < len - 1 ? lo : len - 1;
-          out = (uint16_t)(fbase[f] + (int)local);
+    const size_t r = i / F;
+    const int f = (int)(i - r * F);
+    const float v = X[i];
+    uint16_t local = MISSING_BIN;
+    if (!is_missing_d(v, missing, miss_nan)) {
+      const uint32_t s = foff[f], e = foff[f + 1];
+      const uint32_t len = e - s;
+      if (is_cat[f]) {
+        uint32_t lo = 0, hi = len, found = 0;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          const float c = cuts[s + mid];
+          if (c < v) lo = mid + 1;
+          else if (c > v) hi = mid;
+          else { found = mid; break; }
         }
+        local = (uint16_t)found;
+      } else {
+        uint32_t lo = 0, hi = len;  // partition_point(c <= v)
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
+        }
+        local = (uint16_t)(lo < len - 1 ? lo : len - 1);
       }
     }
-    bins[i] = out;
-    if (f < F) bins_col[(size_t)f * n + r] = out;
+    bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (uint16_t)rmiss[f] : (uint16_t)(rbase[f] + (int)local);
+    bins_col[(size_t)f * n + r] = local;
   }
 }
 
@@ -512,24 +512,53 @@ int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t
     g->max_feature_bins = std::max(g->max_feature_bins, m);
     if (hcat[f]) g->has_categorical = 1;
   }
+  return ghist_bin(ctx, d_X, g);
+}
+
+// The rest of the index from the host cuts (h_foff, h_cuts, h_is_cat): device
+// copies of the cuts, the histogram layout and the bin codes of every entry.
+int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
+  const size_t n = g->n, F = g->F;
+  const float missing = g->missing;
+  cudaStream_t st = ctx->stream;
   g->total_bins = g->h_cuts.size();
+  g->max_feature_bins = 0;
+  g->has_categorical = 0;
+  for (size_t f = 0; f < F; ++f) {
+    g->max_feature_bins = std::max(g->max_feature_bins, (int)(g->h_foff[f + 1] - g->h_foff[f]));
+    if (g->h_is_cat[f]) g->has_categorical = 1;
+  }
+  if (!g->is_cat.p) {
+    SB_TRY(g->is_cat.alloc(ctx, F));
+    SB_CUDA(cudaMemcpyAsync(g->is_cat.p, g->h_is_cat.data(), F, cudaMemcpyHostToDevice, st));
+  }
   SB_TRY(g->foff.alloc(ctx, F + 1));
   SB_TRY(g->cuts.alloc(ctx, g->total_bins));
   SB_CUDA(cudaMemcpyAsync(g->foff.p, g->h_foff.data(), (F + 1) * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(g->cuts.p, g->h_cuts.data(), g->total_bins * 4, cudaMemcpyHostToDevice, st));
 
-  SB_TRY(hist_prepare(ctx, g));  // feature tiles fix the bin codes
+  SB_TRY(hist_prepare(ctx, g));  // the histogram layout fixes the row codes
+  // feature-major codes are the local bins themselves
+  const std::vector<int> zeros(F, 0), miss(F, (int)MISSING_BIN);
   SB_TRY(g->fbase.alloc(ctx, F));
   SB_TRY(g->fmiss.alloc(ctx, F));
-  SB_CUDA(cudaMemcpyAsync(g->fbase.p, g->h_fbase.data(), F * 4, cudaMemcpyHostToDevice, st));
-  SB_CUDA(cudaMemcpyAsync(g->fmiss.p, g->h_fmiss.data(), F * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(g->fbase.p, zeros.data(), F * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(g->fmiss.p, miss.data(), F * 4, cudaMemcpyHostToDevice, st));
+  DBuf<int> rpos, rbase, rmiss;
+  SB_TRY(rpos.alloc(ctx, F));
+  SB_TRY(rbase.alloc(ctx, F));
+  SB_TRY(rmiss.alloc(ctx, F));
+  SB_CUDA(cudaMemcpyAsync(rpos.p, g->h_rpos.data(), F * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(rbase.p, g->h_rbase.data(), F * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(rmiss.p, g->h_rmiss.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_TRY(g->bins.alloc(ctx, n * g->Fp));
   SB_TRY(g->bins_col.alloc(ctx, n * F));
-  size_t total = n * g->Fp;
-  unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 32);
-  SB_LAUNCH(ctx, k_bin, blocks, 256, 0, d_X, n, (int)F, (int)g->Fp, missing, g->foff.p, g->cuts.p,
-            g->is_cat.p, g->fbase.p, g->fmiss.p, g->bins.p, g->bins_col.p);
-  SB_CUDA(cudaStreamSynchronize(st));  // temporaries are released on return
+  SB_CUDA(cudaMemsetAsync(g->bins.p, 0xFF, g->bins.bytes(), st));  // unused positions: 0xFFFF
+  const size_t total = n * F;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 32);
+  SB_LAUNCH(ctx, k_bin, blocks, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+            g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
+  SB_CUDA(cudaStreamSynchronize(st));  // temporaries and host vectors are released on return
   return SB_OK;
 }
 
@@ -591,14 +620,11 @@ int sb_ghist_cuts(const sb_ghist* g, uint32_t* feature_offset, float* cut_values
 int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins) {
   SB_REQUIRE(g && local_bins, SB_ERR_INVALID_ARG, "NULL argument");
   SB_CUDA(cudaSetDevice(g->ctx->device));
-  SB_CUDA(cudaMemcpy2DAsync(local_bins, g->F * 2, g->bins.p, g->Fp * 2, g->F * 2, g->n,
-                            cudaMemcpyDeviceToHost, g->ctx->stream));
+  std::vector<uint16_t> col(g->n * g->F);  // feature-major local bins
+  SB_CUDA(cudaMemcpyAsync(col.data(), g->bins_col.p, col.size() * 2, cudaMemcpyDeviceToHost, g->ctx->stream));
   SB_CUDA(cudaStreamSynchronize(g->ctx->stream));
-  for (size_t r = 0; r < g->n; ++r)  // tile-relative codes -> local bins
-    for (size_t f = 0; f < g->F; ++f) {
-      uint16_t& c = local_bins[r * g->F + f];
-      c = (int)c == g->h_fmiss[f] ? sb::MISSING_BIN : (uint16_t)((int)c - g->h_fbase[f]);
-    }
+  for (size_t f = 0; f < g->F; ++f)
+    for (size_t r = 0; r < g->n; ++r) local_bins[r * g->F + f] = col[f * g->n + r];
   return SB_OK;
 }
 

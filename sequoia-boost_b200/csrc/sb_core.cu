@@ -89,7 +89,7 @@ void sb_train_params_default(sb_train_params* p) {  // config/params.rs:153-186
   p->max_leaves = 0;
   p->grow_policy = SB_GROW_DEPTHWISE;
   p->max_bin = 256;
-  p->hist_precision = SB_HIST_FP32;
+  p->hist_precision = SB_HIST_FIXED;  // exact, run-to-run deterministic histograms
   p->quantize_bits = 0;
 }
 
@@ -129,6 +129,8 @@ int sb_train_params_validate(const sb_train_params* p) {  // config/params.rs:19
              SB_ERR_INVALID_ARG, "unknown hist_precision %d", p->hist_precision);
   SB_REQUIRE(p->quantize_bits == 0 || (p->quantize_bits >= 8 && p->quantize_bits <= 23),
              SB_ERR_INVALID_ARG, "quantize_bits must be 0 or in [8, 23]");
+  SB_REQUIRE(p->tree_method == SB_TREE_HIST || p->tree_method == SB_TREE_APPROX, SB_ERR_INVALID_ARG,
+             "unknown tree_method %d", p->tree_method);
   // Limits of this backend (documented): depthwise trees up to depth 12 (the
   // level histograms are preallocated), lossguide up to 4096 leaves.
   if (p->grow_policy == SB_GROW_DEPTHWISE)

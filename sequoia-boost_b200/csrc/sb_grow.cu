@@ -220,6 +220,54 @@ __device__ __forceinline__ float sigmoidf_ref(float x) {  // classification.rs:7
 }
 
 // ---------------------------------------------------------------- K3
+// Objective::gradient for one row's K margins `mr` (regression.rs:18-85,
+// classification.rs:50-71, multiclass.rs:14-30 and :64-91), with explicit
+// f32 rounding so that no multiply-add is contracted. `w0` is the row's
+// weight (1 when the caller has none, `has_w` = 0). emit(c, g, h) receives
+// the pair of output c.
+template <typename Emit>
+__device__ __forceinline__ void row_gradient(int objective, int K, float spw, const float* mr, float y,
+                                             float w0, bool has_w, Emit emit) {
+  if (K == 1) {
+    const float m = mr[0];
+    float g, h;
+    if (objective == SB_OBJ_SQUARED_ERROR) {  // regression.rs:18-40
+      const float d = __fsub_rn(m, y);
+      g = has_w ? __fmul_rn(d, w0) : d;
+      h = has_w ? w0 : 1.0f;
+    } else if (objective == SB_OBJ_PSEUDOHUBER) {  // regression.rs:51-85
+      const float d = __fsub_rn(m, y);
+      const float s = __fadd_rn(1.0f, __fmul_rn(d, d));
+      const float sq = __fsqrt_rn(s);
+      g = __fmul_rn(__fdiv_rn(d, sq), w0);
+      h = __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(s, sq)), w0);
+    } else {  // logistic, classification.rs:50-71
+      const float p = sigmoidf_ref(m);
+      float w = w0;
+      if (y == 1.0f) w = __fmul_rn(w, spw);
+      g = __fmul_rn(__fsub_rn(p, y), w);
+      h = __fmul_rn(fmaxf(__fmul_rn(p, __fsub_rn(1.0f, p)), 1e-16f), w);
+    }
+    emit(0, g, h);
+    return;
+  }
+  // softmax, multiclass.rs:14-30, :64-91
+  float mx = -INFINITY;
+  for (int c = 0; c < K; ++c)
+    if (mr[c] > mx) mx = mr[c];
+  float sum = 0.0f;
+  for (int c = 0; c < K; ++c) sum = __fadd_rn(sum, expf(__fsub_rn(mr[c], mx)));
+  const float inv = __fdiv_rn(1.0f, sum);
+  const uint32_t label = f32_as_u32(y);  // `as usize` saturates: negative and NaN labels are class 0
+  for (int c = 0; c < K; ++c) {
+    const float p = __fmul_rn(expf(__fsub_rn(mr[c], mx)), inv);
+    const float target = ((uint32_t)c == label) ? 1.0f : 0.0f;
+    const float g = __fmul_rn(__fsub_rn(p, target), w0);
+    const float h = fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(2.0f, p), __fsub_rn(1.0f, p)), w0), 1e-16f);
+    emit(c, g, h);
+  }
+}
+
 __global__ void k_gradient(BState S) {
   const unsigned long long round = *S.round + S.round_base;
   const uint64_t rk = sb_round_key(S.seed, round);
@@ -234,50 +282,14 @@ __global__ void k_gradient(BState S) {
       const float y = S.labels[r];
       if (S.apply_delta)  // the previous tree's leaf values (train.rs:326-328)
         for (int c = 0; c < K; ++c) S.margin[r * K + c] = __fadd_rn(S.margin[r * K + c], S.delta[r * K + c]);
-      if (K == 1) {
-        const float m = S.margin[r];
-        float g, h;
-        if (S.objective == SB_OBJ_SQUARED_ERROR) {  // regression.rs:18-40
-          float d = __fsub_rn(m, y);
-          g = S.weights ? __fmul_rn(d, w0) : d;
-          h = S.weights ? w0 : 1.0f;
-        } else if (S.objective == SB_OBJ_PSEUDOHUBER) {  // regression.rs:51-85
-          float d = __fsub_rn(m, y);
-          float s = __fadd_rn(1.0f, __fmul_rn(d, d));
-          float sq = __fsqrt_rn(s);
-          g = __fmul_rn(__fdiv_rn(d, sq), w0);
-          h = __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(s, sq)), w0);
-        } else {  // logistic, classification.rs:50-71
-          float p = sigmoidf_ref(m);
-          float w = w0;
-          if (y == 1.0f) w = __fmul_rn(w, S.spw);
-          g = __fmul_rn(__fsub_rn(p, y), w);
-          h = __fmul_rn(fmaxf(__fmul_rn(p, __fsub_rn(1.0f, p)), 1e-16f), w);
-        }
-        S.gpair[r] = make_float2(g, h);
-        mg[0] = fmaxf(mg[0], fabsf(g));
-        mh[0] = fmaxf(mh[0], fabsf(h));
-      } else {  // softmax, multiclass.rs:14-30, :64-91
-        const float* mr = S.margin + r * K;
-        float mx = -INFINITY;
-        for (int c = 0; c < K; ++c)
-          if (mr[c] > mx) mx = mr[c];
-        float sum = 0.0f;
-        for (int c = 0; c < K; ++c) sum = __fadd_rn(sum, expf(__fsub_rn(mr[c], mx)));
-        const float inv = __fdiv_rn(1.0f, sum);
-        const int label = (int)y;
-        for (int c = 0; c < K; ++c) {
-          float p = __fmul_rn(expf(__fsub_rn(mr[c], mx)), inv);
-          float target = (c == label) ? 1.0f : 0.0f;
-          float g = __fmul_rn(__fsub_rn(p, target), w0);
-          float h = fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(2.0f, p), __fsub_rn(1.0f, p)), w0), 1e-16f);
-          S.gpair[(size_t)c * S.n + r] = make_float2(g, h);
-          if (c < 16) {
-            mg[c] = fmaxf(mg[c], fabsf(g));
-            mh[c] = fmaxf(mh[c], fabsf(h));
-          }
-        }
-      }
+      row_gradient(S.objective, K, S.spw, S.margin + r * K, y, w0, S.weights != nullptr,
+                   [&](int c, float g, float h) {
+                     S.gpair[(size_t)c * S.n + r] = make_float2(g, h);
+                     if (c < 16) {
+                       mg[c] = fmaxf(mg[c], fabsf(g));
+                       mh[c] = fmaxf(mh[c], fabsf(h));
+                     }
+                   });
     } else {
       for (int c = 0; c < K && c < 16; ++c) {
         float2 v = S.gpair[(size_t)c * S.n + r];
@@ -316,6 +328,19 @@ __global__ void k_gradient(BState S) {
   if (threadIdx.x == 0 && s_kept) atomicAdd(S.kept, s_kept);
   if (S.fixed && threadIdx.x < 2 * K && threadIdx.x < 32 && s_max[threadIdx.x])
     atomicMax(&S.maxabs[threadIdx.x], s_max[threadIdx.x]);
+}
+
+// Objective::gradient over caller-supplied margins (row-major [n][K]),
+// writing the reference's row-major GradPair [n][K] layout.
+__global__ void k_objective_gradient(int objective, int K, float spw, const float* __restrict__ preds,
+                                     const float* __restrict__ labels, const float* __restrict__ weights,
+                                     size_t n, float2* __restrict__ out) {
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (size_t)gridDim.x * blockDim.x) {
+    const float w0 = weights ? weights[r] : 1.0f;
+    row_gradient(objective, K, spw, preds + r * K, labels[r], w0, weights != nullptr,
+                 [&](int c, float g, float h) { out[r * K + c] = make_float2(g, h); });
+  }
 }
 
 // Column subset of node `nid` (sampler.rs:52-70 with sb_sampling.h keys),
@@ -1667,6 +1692,105 @@ int quantize_pairs(sb_ctx* ctx, const float2* d_gp, size_t n, int bits, unsigned
 
 namespace {
 
+// Objective::base_margin / prob_to_margin with TrainingParams::base_score
+// (learner/train.rs:203-210) from host labels and weights.
+float base_margin_of(const sb_train_params* p, const float* labels, const float* weights, size_t n, int K) {
+  float base;
+  if (K > 1) base = 0.0f;
+  else if (p->has_base_score) {
+    float bs = (float)p->base_score;
+    if (p->objective == SB_OBJ_LOGISTIC) {
+      float pp = bs < 1e-6f ? 1e-6f : (bs > 1.0f - 1e-6f ? 1.0f - 1e-6f : bs);
+      base = logf(pp / (1.0f - pp));
+    } else {
+      base = bs;
+    }
+  } else {
+    double mean = 0.0;
+    if (weights) {
+      double num = 0.0, den = 0.0;
+      for (size_t i = 0; i < n; ++i) {
+        num += (double)labels[i] * (double)weights[i];
+        den += (double)weights[i];
+      }
+      mean = den > 0.0 ? num / den : 0.0;
+    } else {
+      double sum = 0.0;
+      for (size_t i = 0; i < n; ++i) sum += (double)labels[i];
+      mean = sum / (double)n;
+    }
+    if (p->objective == SB_OBJ_LOGISTIC) {
+      double pp = mean < 1e-6 ? 1e-6 : (mean > 1.0 - 1e-6 ? 1.0 - 1e-6 : mean);
+      base = (float)log(pp / (1.0 - pp));
+    } else {
+      base = (float)mean;
+    }
+  }
+  return base;
+}
+
+// ----------------------------------------------------- tree_method=approx
+// Row subset of round `round` with the hist path's keys (sample_rows,
+// train.rs:465-475): rows[r] = r, flagged UNSAMPLED when not drawn.
+__global__ void k_approx_rows(uint64_t seed, unsigned long long round, double subsample, size_t n,
+                              uint32_t* __restrict__ rows, unsigned int* __restrict__ kept) {
+  const uint64_t rk = sb_round_key(seed, round);
+  unsigned int c = 0;
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    const bool keep = subsample >= 1.0 || sb_u01(sb_row_draw(rk, r)) < subsample;
+    rows[r] = (uint32_t)r | (keep ? 0u : UNSAMPLED);
+    c += keep ? 1u : 0u;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(kept, c);
+}
+
+__global__ void k_approx_fallback(uint64_t seed, unsigned long long round, size_t n, uint32_t* __restrict__ rows,
+                                  const unsigned int* __restrict__ kept) {
+  if (*kept == 0) rows[sb_row_fallback(sb_round_key(seed, round), n)] &= ~UNSAMPLED;  // train.rs:472-474
+}
+
+// Class k's gradient pairs and hessians out of the row-major [n][K] pairs.
+__global__ void k_class_column(const float2* __restrict__ gp, size_t n, int K, int k, float2* __restrict__ out,
+                               float* __restrict__ hess) {
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = gp[r * K + k];
+    out[r] = v;
+    hess[r] = v.y;
+  }
+}
+
+// margin[r][k] += f32(leaf * eta) of the row's leaf in one tree, routed on
+// the raw values (RegTree::predict_row, regtree.rs:213-242; train.rs:323-328).
+__global__ void k_add_tree(const sb_node* __restrict__ nodes, const uint32_t* __restrict__ cats,
+                           const float* __restrict__ X, size_t n, int F, float missing, int K, int k, float eta,
+                           float* __restrict__ margin) {
+  const bool miss_nan = isnan(missing);
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+    int nid = 0;
+    while (nodes[nid].left >= 0) {
+      const sb_node nd = nodes[nid];
+      const float v = X[r * F + nd.split_feature];
+      bool left;
+      if (miss_nan ? isnan(v) : v == missing) left = nd.default_left != 0;
+      else if (nd.is_categorical) {
+        const uint32_t c = f32_as_u32(v);
+        left = false;
+        for (uint32_t i = nd.cat_begin; i < nd.cat_end; ++i)
+          if (cats[i] == c) {
+            left = true;
+            break;
+          }
+      } else {
+        left = v < nd.split_cond;
+      }
+      nid = left ? nd.left : nd.right;
+    }
+    float* m = margin + r * K + k;
+    *m = __fadd_rn(*m, __fmul_rn(nodes[nid].leaf_value, eta));
+  }
+}
+
 int booster_alloc_trees(sb_booster* b, int need) {
   if (need <= b->tree_cap) return SB_OK;
   int cap = std::max(need, b->tree_cap * 2);
@@ -2196,14 +2320,112 @@ int booster_run(sb_booster* b, int n_rounds) {
 
 }  // namespace sb
 
+namespace sb {
+
+// train_impl for tree_method=approx (learner/train.rs:46-53, 276-338): each
+// round, per class, hessian-weighted cuts of that class's hessians, the
+// matrix re-binned with them, one tree grown by the hist builder on it, and
+// the margins updated on the raw values.
+int approx_train(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t* ftypes, float missing,
+                 const float* labels, const float* weights, const float* base_margin, const sb_train_params* p,
+                 int rounds, sb_model** out) {
+  cudaStream_t st = ctx->stream;
+  const int K = n_outputs(p->objective, p->num_class);
+  if (weights)
+    for (size_t i = 0; i < n; ++i)
+      SB_REQUIRE(weights[i] >= 0.0f, SB_ERR_UNSUPPORTED, "tree_method=approx needs non-negative weights");
+  ApproxState* A = approx_state_new();
+  std::unique_ptr<ApproxState, void (*)(ApproxState*)> own(A, approx_state_free);
+  SB_TRY(approx_prepare(ctx, d_X, n, F, ftypes, missing, p->max_bin, A));
+  const float base = base_margin_of(p, labels, weights, n, K);
+  std::vector<float> m0(n * K, base);
+  if (base_margin) std::memcpy(m0.data(), base_margin, n * K * sizeof(float));
+  DBuf<float> d_y, d_w, d_margin, d_hess;
+  DBuf<float2> d_gp, d_gk;
+  DBuf<unsigned int> d_kept;
+  SB_TRY(d_y.alloc(ctx, n));
+  if (weights) SB_TRY(d_w.alloc(ctx, n));
+  SB_TRY(d_margin.alloc(ctx, n * K));
+  SB_TRY(d_hess.alloc(ctx, n));
+  SB_TRY(d_gp.alloc(ctx, n * K));
+  SB_TRY(d_gk.alloc(ctx, n));
+  SB_TRY(d_kept.alloc(ctx, 1));
+  SB_CUDA(cudaMemcpyAsync(d_y.p, labels, n * 4, cudaMemcpyHostToDevice, st));
+  if (weights) SB_CUDA(cudaMemcpyAsync(d_w.p, weights, n * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_margin.p, m0.data(), n * K * 4, cudaMemcpyHostToDevice, st));
+  std::unique_ptr<sb_model> mdl(new sb_model);
+  mdl->ctx = ctx;
+  mdl->base_score = base;
+  mdl->num_class = p->num_class;
+  mdl->n_features = (int)F;
+  mdl->objective = p->objective;
+  sb_train_params q = *p;  // the trees' builder params (its gradients come from here)
+  q.objective = SB_OBJ_SQUARED_ERROR;
+  q.num_class = 0;
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
+  const float eta = (float)p->eta;
+  for (int r = 0; r < rounds; ++r) {
+    SB_LAUNCH(ctx, k_objective_gradient, blocks, 256, 0, p->objective, K, (float)p->scale_pos_weight, d_margin.p,
+              d_y.p, d_w.p, n, d_gp.p);
+    for (int k = 0; k < K; ++k) {
+      SB_LAUNCH(ctx, k_class_column, blocks, 256, 0, d_gp.p, n, K, k, d_gk.p, d_hess.p);
+      sb_ghist g;
+      g.ctx = ctx;
+      g.n = n;
+      g.F = F;
+      g.max_bin = p->max_bin;
+      g.missing = missing;
+      SB_TRY(approx_cuts(A, d_hess.p, &g));  // HistCuts::from_dmatrix_weighted
+      SB_TRY(ghist_bin(ctx, d_X, &g));       // GHistIndex::from_dmatrix
+      sb_booster b;
+      SB_TRY(booster_init(&b, ctx, &g, &q, 1, true));
+      SB_CUDA(cudaMemsetAsync(d_kept.p, 0, 4, st));
+      SB_LAUNCH(ctx, k_approx_rows, blocks, 256, 0, p->seed, (unsigned long long)r, p->subsample, n, b.d_rows0.p,
+                d_kept.p);
+      SB_LAUNCH(ctx, k_approx_fallback, 1, 1, 0, p->seed, (unsigned long long)r, n, b.d_rows0.p, d_kept.p);
+      SB_CUDA(cudaMemcpyAsync(b.d_gpair.p, d_gk.p, n * 8, cudaMemcpyDeviceToDevice, st));
+      b.S.round_base = (unsigned long long)r;  // column sampling of class k in round r
+      b.S.k_base = k;
+      SB_TRY(booster_set_eval_smem(&b));
+      SB_TRY(booster_round(&b));
+      SB_LAUNCH(ctx, k_add_tree, blocks, 256, 0, b.d_out_nodes.p, b.d_out_cats.p, d_X, n, (int)F, missing, K, k,
+                eta, d_margin.p);
+      int nn = 0, nc = 0;
+      std::vector<sb_node> nodes(b.maxn);
+      SB_CUDA(cudaMemcpyAsync(&nn, b.d_out_nnodes.p, 4, cudaMemcpyDeviceToHost, st));
+      SB_CUDA(cudaMemcpyAsync(&nc, b.d_out_ncats.p, 4, cudaMemcpyDeviceToHost, st));
+      SB_CUDA(cudaMemcpyAsync(nodes.data(), b.d_out_nodes.p, b.maxn * sizeof(sb_node), cudaMemcpyDeviceToHost, st));
+      std::vector<uint32_t> cats(b.S.cat_cap);
+      if (b.S.cat_cap)
+        SB_CUDA(cudaMemcpyAsync(cats.data(), b.d_out_cats.p, b.S.cat_cap * 4, cudaMemcpyDeviceToHost, st));
+      SB_CUDA(cudaStreamSynchronize(st));
+      HostTree t;
+      t.nodes.assign(nodes.begin(), nodes.begin() + nn);
+      t.cats.assign(cats.begin(), cats.begin() + nc);
+      for (sb_node& nd : t.nodes)  // scale_leaves(eta), regtree.rs:201-207
+        if (nd.left < 0) nd.leaf_value = nd.leaf_value * eta;
+      mdl->trees.push_back(std::move(t));
+      mdl->weights.push_back(1.0f);
+    }
+  }
+  SB_CUDA(cudaStreamSynchronize(st));
+  *out = mdl.release();
+  return SB_OK;
+}
+
+}  // namespace sb
+
 extern "C" {
 
 int sb_booster_create(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p, const float* labels,
                       const float* weights, const float* base_margin, sb_booster** out) {
   using namespace sb;
   SB_REQUIRE(ctx && g && p && labels && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_SAME_DEVICE(ctx, g);
   *out = nullptr;
   SB_TRY(sb_train_params_validate(p));
+  SB_REQUIRE(p->tree_method == SB_TREE_HIST, SB_ERR_UNSUPPORTED,
+             "a booster trains tree_method=hist; tree_method=approx trains through sb_train");
   SB_CUDA(cudaSetDevice(ctx->device));
   const int K = n_outputs(p->objective, p->num_class);
   const size_t n = g->n;
@@ -2217,38 +2439,7 @@ int sb_booster_create(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p, 
     delete b;
     return s;
   }
-  // base margin, train.rs:203-210 (host: the labels are on the host here)
-  float base;
-  if (K > 1) base = 0.0f;
-  else if (p->has_base_score) {
-    float bs = (float)p->base_score;
-    if (p->objective == SB_OBJ_LOGISTIC) {
-      float pp = bs < 1e-6f ? 1e-6f : (bs > 1.0f - 1e-6f ? 1.0f - 1e-6f : bs);
-      base = logf(pp / (1.0f - pp));
-    } else {
-      base = bs;
-    }
-  } else {
-    double mean = 0.0;
-    if (weights) {
-      double num = 0.0, den = 0.0;
-      for (size_t i = 0; i < n; ++i) {
-        num += (double)labels[i] * (double)weights[i];
-        den += (double)weights[i];
-      }
-      mean = den > 0.0 ? num / den : 0.0;
-    } else {
-      double sum = 0.0;
-      for (size_t i = 0; i < n; ++i) sum += (double)labels[i];
-      mean = sum / (double)n;
-    }
-    if (p->objective == SB_OBJ_LOGISTIC) {
-      double pp = mean < 1e-6 ? 1e-6 : (mean > 1.0 - 1e-6 ? 1.0 - 1e-6 : mean);
-      base = (float)log(pp / (1.0 - pp));
-    } else {
-      base = (float)mean;
-    }
-  }
+  const float base = base_margin_of(p, labels, weights, n, K);
   b->base_score = base;
   std::vector<float> m(n * K, base);  // init_margin, train.rs:496-511
   if (base_margin) std::memcpy(m.data(), base_margin, n * K * sizeof(float));
@@ -2389,11 +2580,45 @@ int sb_booster_stats_reset(sb_booster* b) {
   return SB_OK;
 }
 
+int sb_objective_gradient(sb_ctx* ctx, int objective, int num_class, double scale_pos_weight,
+                          const float* preds, const float* labels, const float* weights, size_t n_rows,
+                          sb_gradpair* out) {
+  using namespace sb;
+  SB_REQUIRE(ctx && labels && out && (n_rows == 0 || preds), SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(objective >= SB_OBJ_SQUARED_ERROR && objective <= SB_OBJ_SOFTPROB, SB_ERR_INVALID_ARG,
+             "unknown objective %d", objective);
+  const bool multi = objective == SB_OBJ_SOFTMAX || objective == SB_OBJ_SOFTPROB;
+  SB_REQUIRE(!multi || num_class >= 2, SB_ERR_INVALID_ARG,
+             "invalid parameter `num_class`: multiclass objectives require num_class >= 2");
+  SB_REQUIRE(scale_pos_weight > 0.0, SB_ERR_INVALID_ARG, "invalid parameter `scale_pos_weight`: must be > 0");
+  if (n_rows == 0) return SB_OK;
+  SB_CUDA(cudaSetDevice(ctx->device));
+  const int K = n_outputs(objective, num_class);
+  const size_t nk = n_rows * (size_t)K;
+  cudaStream_t st = ctx->stream;
+  DBuf<float> d_p, d_y, d_w;
+  DBuf<float2> d_out;
+  SB_TRY(d_p.alloc(ctx, nk));
+  SB_TRY(d_y.alloc(ctx, n_rows));
+  if (weights) SB_TRY(d_w.alloc(ctx, n_rows));
+  SB_TRY(d_out.alloc(ctx, nk));
+  SB_CUDA(cudaMemcpyAsync(d_p.p, preds, nk * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(d_y.p, labels, n_rows * 4, cudaMemcpyHostToDevice, st));
+  if (weights) SB_CUDA(cudaMemcpyAsync(d_w.p, weights, n_rows * 4, cudaMemcpyHostToDevice, st));
+  const unsigned blocks = (unsigned)std::min<size_t>((n_rows + 255) / 256, (size_t)ctx->num_sms * 16);
+  SB_LAUNCH(ctx, k_objective_gradient, blocks, 256, 0, objective, K, (float)scale_pos_weight, d_p.p, d_y.p,
+            d_w.p, n_rows, d_out.p);
+  SB_CUDA(cudaMemcpyAsync(out, d_out.p, nk * 8, cudaMemcpyDeviceToHost, st));
+  SB_CUDA(cudaStreamSynchronize(st));
+  return SB_OK;
+}
+
 int sb_tree_build(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p, const sb_gradpair* gpair,
                   size_t n, const uint32_t* rows, size_t m, uint64_t round, uint32_t k,
                   int32_t* row_leaf, sb_model** out) {
   using namespace sb;
   SB_REQUIRE(ctx && g && p && gpair && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_SAME_DEVICE(ctx, g);
   SB_REQUIRE(m == 0 || rows, SB_ERR_INVALID_ARG, "rows is NULL");
   SB_REQUIRE(n == g->n, SB_ERR_DIMENSION, "dimension mismatch: gpair length expected %zu, got %zu",
              g->n, n);
@@ -2461,6 +2686,16 @@ int sb_train(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols, const ui
   SB_REQUIRE(ctx && X && labels && p && out, SB_ERR_INVALID_ARG, "NULL argument");
   SB_REQUIRE(num_boost_round >= 0, SB_ERR_INVALID_ARG, "negative num_boost_round");
   SB_TRY(sb_train_params_validate(p));
+  if (p->tree_method == SB_TREE_APPROX) {
+    SB_REQUIRE(n_rows > 0 && n_cols > 0, SB_ERR_INVALID_ARG, "empty dataset: zero rows or columns");
+    SB_CUDA(cudaSetDevice(ctx->device));
+    *out = nullptr;
+    sb::DBuf<float> dX;
+    SB_TRY(dX.alloc(ctx, n_rows * n_cols));
+    SB_CUDA(cudaMemcpyAsync(dX.p, X, dX.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    return sb::approx_train(ctx, dX.p, n_rows, n_cols, feature_types, missing, labels, weights, base_margin, p,
+                            num_boost_round, out);
+  }
   sb_ghist* g = nullptr;
   SB_TRY(sb_ghist_create(ctx, X, n_rows, n_cols, feature_types, missing, p->max_bin, &g));
   sb_booster* b = nullptr;

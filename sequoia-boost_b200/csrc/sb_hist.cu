@@ -20,6 +20,10 @@
 // Each feature also owns one extra "missing" bin (index total_bins + f), so a
 // node's missing-value statistics are summed directly instead of being
 // recovered as total - present.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+
 #include "sb_internal.cuh"
 
 namespace sb {
@@ -32,7 +36,9 @@ constexpr int ROWS_PER_WARP = 8;        // rows in flight per warp
 struct HistDev {
   const uint16_t* bins;
   const uint32_t* foff;
-  size_t Fp;
+  size_t Fp;             // row stride of bins (u16)
+  const int* ent_gbin;   // LANES: (entry, lane) -> histogram bin, per tile
+  const int* slot_feat;  // LANES: feature of each code position of a row
   size_t n;              // gradient column stride
   int total_bins;
   const void* gpair;
@@ -227,6 +233,195 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
   }
 }
 
+// LANES layout (see sb_internal.cuh): lane l of every warp owns the features
+// in its `S` code positions of the tile, and entry e of lane l lives at word
+// e * 32 + l of each plane, so every shared atomic instruction of a warp hits
+// 32 different banks. A row costs one S x u16 load per lane and 2 * S shared
+// atomic instructions per warp; the partial is flushed through the tile's
+// (entry, lane) -> histogram-bin table.
+template <int S> struct Codes;
+template <> struct Codes<1> {
+  using T = unsigned short;
+  __device__ static T none() { return 0xFFFFu; }
+  __device__ static int get(T v, int) { return (int)v; }
+};
+template <> struct Codes<2> {
+  using T = unsigned int;
+  __device__ static T none() { return 0xFFFFFFFFu; }
+  __device__ static int get(T v, int s) { return (int)((v >> (16 * s)) & 0xFFFFu); }
+};
+template <> struct Codes<4> {
+  using T = uint2;
+  __device__ static T none() { return make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu); }
+  __device__ static int get(T v, int s) {
+    const unsigned w = s < 2 ? v.x : v.y;
+    return (int)((w >> (16 * (s & 1))) & 0xFFFFu);
+  }
+};
+
+template <bool FIXED, int S>
+__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_lanes(HistDev a) {
+  using C = Codes<S>;
+  using CT = typename C::T;
+  extern __shared__ unsigned long long sh_u64[];
+  unsigned* sh_g = reinterpret_cast<unsigned*>(sh_u64);
+  __shared__ double s_tot_d[2];
+  __shared__ unsigned long long s_tot_u[2];
+
+  const int count = *a.count;
+  if (count <= 0) return;
+  const uint64_t W = a.prefix[count];
+  if (W == 0) return;
+  const uint64_t U = W * (uint64_t)a.ntiles;
+  const uint64_t lo = U * blockIdx.x / gridDim.x, hi = U * (blockIdx.x + 1) / gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+  uint64_t u = lo;
+  while (u < hi) {
+    const int t = (int)(u / W);
+    const uint64_t pos = u - (uint64_t)t * W;
+    const int it = find_item(a.prefix, count, pos);
+    const HistItem item = a.items[it];
+    const uint64_t item_lo = a.prefix[it], item_hi = a.prefix[it + 1];
+    uint64_t piece_hi_u = (uint64_t)t * W + item_hi;
+    if (piece_hi_u > hi) piece_hi_u = hi;
+    uint64_t n_pos = piece_hi_u - u;
+    if (FIXED && n_pos > a.flush_rows) n_pos = a.flush_rows;
+    const uint32_t pbeg = item.begin + (uint32_t)(pos - item_lo);
+    const uint32_t pend = pbeg + (uint32_t)n_pos;
+    const FeatureTile tile = a.tiles[t];
+    const int words = 32 * tile.E;  // per plane
+    unsigned* sh_h = sh_g + words;
+    const bool want_total = item.root && t == 0;
+
+    // the features of this lane's code positions that the tree's column pool
+    // keeps (unused positions are off)
+    const int slot0 = tile.slot_off + lane * S;
+    bool fon[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int f = a.slot_feat[slot0 + s];
+      bool on = f >= 0;
+      if (on && a.pool_mask && !((a.pool_mask[(size_t)item.k * a.FW + (f >> 5)] >> (f & 31)) & 1u)) on = false;
+      fon[s] = on;
+    }
+    for (int i = threadIdx.x; i < 2 * words; i += blockDim.x) sh_g[i] = 0u;
+    if (threadIdx.x < 2) {
+      s_tot_d[threadIdx.x] = 0.0;
+      s_tot_u[threadIdx.x] = 0ull;
+    }
+    __syncthreads();
+
+    double tg = 0.0, th = 0.0;
+    long long tqg = 0;
+    unsigned long long tqh = 0;
+    unsigned int nsampled = 0;
+    const size_t gcol = (size_t)item.k * a.n;
+    const uint16_t* bins_lane = a.bins + slot0;
+    const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
+    uint32_t p = pbeg + warp * ROWS_PER_WARP;
+    uint32_t next_rid = UNSAMPLED;
+    if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
+    for (; p < pend; p += stride) {
+      const uint32_t my_rid = next_rid;
+      const uint32_t pn = p + stride + lane;
+      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
+      const bool my_use = lane < ROWS_PER_WARP && !(my_rid & UNSAMPLED);
+      uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
+      if (my_use) {
+        if (FIXED) {
+          const unsigned long long pk =
+              reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          my_g = (uint32_t)(pk >> 32);
+          my_h = (uint32_t)(pk & 0xFFFFFFFFull);
+        } else {
+          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          my_g = __float_as_uint(v.x);
+          my_h = __float_as_uint(v.y);
+        }
+        nsampled++;
+        if (want_total) {
+          if (FIXED) {
+            tqg += (int)my_g;
+            tqh += my_h;
+          } else {
+            tg += (double)__uint_as_float(my_g);
+            th += (double)__uint_as_float(my_h);
+          }
+        }
+      }
+      const unsigned use_mask = __ballot_sync(0xFFFFFFFFu, my_use);
+      CT cv[ROWS_PER_WARP];
+#pragma unroll
+      for (int q = 0; q < ROWS_PER_WARP; ++q) {
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q) & ~UNSAMPLED;
+        cv[q] = ((use_mask >> q) & 1u) ? __ldg(reinterpret_cast<const CT*>(bins_lane + (size_t)id * a.Fp))
+                                       : C::none();
+      }
+#pragma unroll
+      for (int q = 0; q < ROWS_PER_WARP; ++q) {
+        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, my_g, q);
+        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, my_h, q);
+        if (!((use_mask >> q) & 1u)) continue;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          if (!fon[s]) continue;
+          const int w = C::get(cv[q], s) * 32 + lane;
+          if (FIXED) {
+            atomicAdd(reinterpret_cast<int*>(sh_g) + w, (int)vg);
+            atomicAdd(sh_h + w, vh);
+          } else {
+            atomicAdd(reinterpret_cast<float*>(sh_g) + w, __uint_as_float(vg));
+            atomicAdd(reinterpret_cast<float*>(sh_h) + w, __uint_as_float(vh));
+          }
+        }
+      }
+    }
+    if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
+    if (want_total && lane < ROWS_PER_WARP) {
+      if (FIXED) {
+        atomicAdd(&s_tot_u[0], (unsigned long long)tqg);
+        atomicAdd(&s_tot_u[1], tqh);
+      } else {
+        atomicAdd(&s_tot_d[0], tg);
+        atomicAdd(&s_tot_d[1], th);
+      }
+    }
+    __syncthreads();
+    // flush the partial into the node's HBM histogram
+    const int* eg = a.ent_gbin + tile.ent_off;
+    for (int i = threadIdx.x; i < words; i += blockDim.x) {
+      const int gi = eg[i];
+      if (gi < 0) continue;
+      if (FIXED) {
+        const long long gq = (long long)(int)sh_g[i];
+        const unsigned long long hq = sh_h[i];
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(item.out) + 2 * (size_t)gi;
+        if (gq) atomicAdd(o, (unsigned long long)gq);
+        if (hq) atomicAdd(o + 1, hq);
+      } else {
+        const float g = __uint_as_float(sh_g[i]), h = __uint_as_float(sh_h[i]);
+        double* o = reinterpret_cast<double*>(item.out) + 2 * (size_t)gi;
+        if (g != 0.0f) atomicAdd(o, (double)g);
+        if (h != 0.0f) atomicAdd(o + 1, (double)h);
+      }
+    }
+    if (want_total && threadIdx.x == 0) {
+      if (FIXED) {
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(item.total);
+        atomicAdd(o, s_tot_u[0]);
+        atomicAdd(o + 1, s_tot_u[1]);
+      } else {
+        double* o = reinterpret_cast<double*>(item.total);
+        atomicAdd(o, s_tot_d[0]);
+        atomicAdd(o + 1, s_tot_d[1]);
+      }
+    }
+    __syncthreads();
+    u += n_pos;
+  }
+}
+
 __global__ void k_zero_items(const HistItem* __restrict__ items, const int* __restrict__ count,
                              size_t words) {
   int it = blockIdx.y;
@@ -259,10 +454,15 @@ __global__ void k_fixed_to_f64(const longlong2* __restrict__ in, double2* __rest
 
 }  // namespace
 
-int hist_prepare(sb_ctx* ctx, Ghist* g) {
-  size_t budget = ctx->smem_optin > 8192 ? ctx->smem_optin - 4096 : ctx->smem_optin;
+namespace {
+
+// TILED layout: contiguous feature ranges whose bins and missing entries fit
+// the shared-memory budget, at most 128 features (4 per lane), starting at
+// multiples of 4 features.
+int plan_tiled(Ghist* g, size_t budget) {
   g->tiles.clear();
-  size_t F = g->F, f0 = 0, maxb = 0;
+  const size_t F = g->F;
+  size_t f0 = 0, maxb = 0;
   while (f0 < F) {
     size_t f1 = f0;
     while (f1 < F && f1 - f0 < (size_t)MAX_TILE_FEATURES) {
@@ -274,7 +474,7 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
     if (f1 < F && f1 - f0 >= 4) f1 -= (f1 - f0) % 4;  // next tile starts on a multiple of 4
     SB_REQUIRE(f1 == F || (f1 - f0) % 4 == 0, SB_ERR_UNSUPPORTED,
                "features %zu.. need more shared memory than one CTA has", f0);
-    FeatureTile t;
+    FeatureTile t{};
     t.f0 = (int)f0;
     t.f1 = (int)f1;
     t.bin0 = (int)g->h_foff[f0];
@@ -284,22 +484,180 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
     g->tiles.push_back(t);
     f0 = f1;
   }
-  g->h_fbase.assign(F, 0);
-  g->h_fmiss.assign(F, 0);
+  g->layout = HIST_LAYOUT_TILED;
+  g->slots = 0;
+  g->Fp = (F + 7) / 8 * 8;
+  g->h_rpos.assign(F, 0);
+  g->h_rbase.assign(F, 0);
+  g->h_rmiss.assign(F, 0);
   for (const FeatureTile& t : g->tiles)
     for (int f = t.f0; f < t.f1; ++f) {
-      g->h_fbase[f] = (int)g->h_foff[f] - t.bin0;
-      g->h_fmiss[f] = t.nbins + (f - t.f0);
+      g->h_rpos[f] = f;
+      g->h_rbase[f] = (int)g->h_foff[f] - t.bin0;
+      g->h_rmiss[f] = t.nbins + (f - t.f0);
     }
   g->hist_smem_bytes = maxb;
-  SB_TRY(raise_smem_limit((const void*)k_hist<false>, (size_t)maxb));
-  SB_TRY(raise_smem_limit((const void*)k_hist<true>, (size_t)maxb));
   return SB_OK;
 }
 
+// One feature's place in the LANES layout.
+struct LanePlace {
+  int lane, slot, eb;  // lane, code position within the lane, first entry
+};
+
+// Longest-processing-time packing of features [f0, f1) into 32 lanes of
+// `slots` positions with at most `emax` entries (bins + the missing entry)
+// per lane. Returns the largest lane load, or -1 when the features do not fit.
+int pack_lanes(const Ghist* g, size_t f0, size_t f1, int slots, int emax, std::vector<LanePlace>* out) {
+  const size_t m = f1 - f0;
+  if (m > (size_t)32 * slots) return -1;
+  std::vector<int> order(m);
+  for (size_t i = 0; i < m; ++i) order[i] = (int)(f0 + i);
+  auto ent = [&](int f) { return (int)(g->h_foff[f + 1] - g->h_foff[f]) + 1; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ent(a) > ent(b); });
+  int load[32] = {0}, used[32] = {0};
+  out->assign(m, LanePlace{0, 0, 0});
+  int emx = 1;
+  for (int f : order) {
+    int best = -1;
+    for (int l = 0; l < 32; ++l)
+      if (used[l] < slots && (best < 0 || load[l] < load[best])) best = l;
+    if (best < 0 || load[best] + ent(f) > emax) return -1;
+    (*out)[f - f0] = LanePlace{best, used[best]++, load[best]};
+    load[best] += ent(f);
+    emx = std::max(emx, load[best]);
+  }
+  return emx;
+}
+
+// LANES layout: tiles grow feature by feature while their features still pack
+// into the 32 lanes.
+int plan_lanes(Ghist* g, size_t budget, int slots, std::vector<std::vector<LanePlace>>* places) {
+  const size_t F = g->F;
+  const int emax = (int)std::min<size_t>(budget / (2 * 32 * 4), 0xFFFE);
+  std::vector<FeatureTile> tiles;
+  places->clear();
+  size_t f0 = 0;
+  int ent_off = 0;
+  std::vector<LanePlace> cur, best;
+  while (f0 < F) {
+    size_t f1 = f0;
+    int E = -1;
+    while (f1 < F) {
+      int e = pack_lanes(g, f0, f1 + 1, slots, emax, &cur);
+      if (e < 0) break;
+      E = e;
+      best = cur;
+      f1++;
+    }
+    if (f1 == f0) return SB_ERR_UNSUPPORTED;  // one feature's bins exceed a lane
+    FeatureTile t{};
+    t.f0 = (int)f0;
+    t.f1 = (int)f1;
+    t.bin0 = (int)g->h_foff[f0];
+    t.nbins = (int)(g->h_foff[f1] - g->h_foff[f0]);
+    t.E = E;
+    t.ent_off = ent_off;
+    t.slot_off = (int)tiles.size() * 32 * slots;
+    ent_off += 32 * E;
+    tiles.push_back(t);
+    places->push_back(best);
+    f0 = f1;
+  }
+  g->tiles = tiles;
+  return SB_OK;
+}
+
+size_t lanes_smem(const Ghist* g) {
+  size_t m = 0;
+  for (const FeatureTile& t : g->tiles) m = std::max(m, (size_t)t.E * 32 * 4 * 2);
+  return m;
+}
+
+}  // namespace
+
+// Chooses the layout of the histogram's bin codes and its feature tiles. The
+// LANES layout (conflict-free shared atomics) is taken when every feature
+// fits one lane's column and its rows are at most 1.3x the TILED rows (its
+// rows hold 32 lanes x `slots` positions per tile, padded); SB_HIST_LAYOUT
+// = "tiled" or "lanes" in the environment forces one (for measurements).
+int hist_prepare(sb_ctx* ctx, Ghist* g) {
+  const size_t budget = ctx->smem_optin > 8192 ? ctx->smem_optin - 4096 : ctx->smem_optin;
+  const size_t F = g->F;
+  const char* force = std::getenv("SB_HIST_LAYOUT");
+  const bool force_tiled = force && std::strcmp(force, "tiled") == 0;
+  const bool force_lanes = force && std::strcmp(force, "lanes") == 0;
+  const int slots = F <= 32 ? 1 : (F <= 64 ? 2 : 4);
+  std::vector<std::vector<LanePlace>> places;
+  bool lanes = false;
+  if (!force_tiled && plan_lanes(g, budget, slots, &places) == SB_OK) {
+    const size_t lanes_row = g->tiles.size() * 32 * slots;
+    const size_t tiled_row = (F + 7) / 8 * 8;
+    lanes = force_lanes || lanes_row * 10 <= tiled_row * 13;
+  }
+  SB_REQUIRE(!force_lanes || lanes, SB_ERR_UNSUPPORTED, "SB_HIST_LAYOUT=lanes: a feature has too many bins");
+  if (!lanes) {
+    SB_TRY(plan_tiled(g, budget));
+  } else {
+    g->layout = HIST_LAYOUT_LANES;
+    g->slots = slots;
+    g->Fp = g->tiles.size() * 32 * slots;
+    g->h_rpos.assign(F, 0);
+    g->h_rbase.assign(F, 0);
+    g->h_rmiss.assign(F, 0);
+    size_t ent_total = 0;
+    for (const FeatureTile& t : g->tiles) ent_total += (size_t)32 * t.E;
+    std::vector<int> eg(ent_total, -1), sf(g->Fp, -1);
+    for (size_t ti = 0; ti < g->tiles.size(); ++ti) {
+      const FeatureTile& t = g->tiles[ti];
+      for (int f = t.f0; f < t.f1; ++f) {
+        const LanePlace& pl = places[ti][f - t.f0];
+        const int nb = (int)(g->h_foff[f + 1] - g->h_foff[f]);
+        g->h_rpos[f] = t.slot_off + pl.lane * slots + pl.slot;
+        g->h_rbase[f] = pl.eb;
+        g->h_rmiss[f] = pl.eb + nb;
+        sf[g->h_rpos[f]] = f;
+        for (int b = 0; b < nb; ++b) eg[t.ent_off + (size_t)(pl.eb + b) * 32 + pl.lane] = (int)g->h_foff[f] + b;
+        eg[t.ent_off + (size_t)(pl.eb + nb) * 32 + pl.lane] = (int)(g->total_bins + f);
+      }
+    }
+    SB_TRY(g->ent_gbin.alloc(ctx, eg.size()));
+    SB_TRY(g->slot_feat.alloc(ctx, sf.size()));
+    SB_CUDA(cudaMemcpyAsync(g->ent_gbin.p, eg.data(), eg.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    SB_CUDA(cudaMemcpyAsync(g->slot_feat.p, sf.data(), sf.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    // the pageable copies above must finish before the vectors go away
+    SB_CUDA(cudaStreamSynchronize(ctx->stream));
+    g->hist_smem_bytes = lanes_smem(g);
+  }
+  SB_TRY(raise_smem_limit((const void*)k_hist<false>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist<true>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 1>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 1>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 2>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 2>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 4>, g->hist_smem_bytes));
+  SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 4>, g->hist_smem_bytes));
+  return SB_OK;
+}
+
+namespace {
+
+const void* hist_kernel(const Ghist* g, bool fixed) {
+  if (g->layout == HIST_LAYOUT_LANES) {
+    switch (g->slots) {
+      case 1: return fixed ? (const void*)k_hist_lanes<true, 1> : (const void*)k_hist_lanes<false, 1>;
+      case 2: return fixed ? (const void*)k_hist_lanes<true, 2> : (const void*)k_hist_lanes<false, 2>;
+      default: return fixed ? (const void*)k_hist_lanes<true, 4> : (const void*)k_hist_lanes<false, 4>;
+    }
+  }
+  return fixed ? (const void*)k_hist<true> : (const void*)k_hist<false>;
+}
+
+}  // namespace
+
 int hist_grid(sb_ctx* ctx, const Ghist* g) {
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist<true>, HIST_THREADS,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_kernel(g, true), HIST_THREADS,
                                                 g->hist_smem_bytes);
   if (per_sm < 1) per_sm = 1;
   return ctx->num_sms * per_sm;
@@ -310,6 +668,8 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.bins = L.g->bins.p;
   a.foff = L.g->foff.p;
   a.Fp = L.g->Fp;
+  a.ent_gbin = L.g->ent_gbin.p;
+  a.slot_feat = L.g->slot_feat.p;
   a.n = L.g->n;
   a.total_bins = (int)L.g->total_bins;
   a.gpair = L.gpair;
@@ -322,9 +682,17 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.rows_done = L.rows_done;
   a.pool_mask = L.pool_mask;
   a.FW = (int)((L.g->F + 31) / 32);
-  int grid = hist_grid(ctx, L.g);
-  if (L.fixed) SB_LAUNCH(ctx, k_hist<true>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
-  else SB_LAUNCH(ctx, k_hist<false>, grid, HIST_THREADS, L.g->hist_smem_bytes, a);
+  const int grid = hist_grid(ctx, L.g);
+  const size_t sm = L.g->hist_smem_bytes;
+  void (*kern)(HistDev) = L.fixed ? k_hist<true> : k_hist<false>;
+  if (L.g->layout == HIST_LAYOUT_LANES) {
+    switch (L.g->slots) {
+      case 1: kern = L.fixed ? k_hist_lanes<true, 1> : k_hist_lanes<false, 1>; break;
+      case 2: kern = L.fixed ? k_hist_lanes<true, 2> : k_hist_lanes<false, 2>; break;
+      default: kern = L.fixed ? k_hist_lanes<true, 4> : k_hist_lanes<false, 4>;
+    }
+  }
+  SB_LAUNCH(ctx, kern, grid, HIST_THREADS, sm, a);
   return SB_OK;
 }
 
@@ -350,6 +718,7 @@ int sb_hist_build(sb_ctx* ctx, const sb_ghist* g, const uint32_t* rows, size_t m
                   sb_gradstats* out, size_t total_bins) {
   using namespace sb;
   SB_REQUIRE(ctx && g && gpair && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_SAME_DEVICE(ctx, g);
   SB_REQUIRE(m == 0 || rows, SB_ERR_INVALID_ARG, "rows is NULL");
   SB_REQUIRE(total_bins == g->total_bins, SB_ERR_DIMENSION,
              "dimension mismatch: out length expected %zu, got %zu", g->total_bins, total_bins);

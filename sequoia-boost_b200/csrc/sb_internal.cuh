@@ -113,30 +113,51 @@ constexpr uint16_t MISSING_BIN = 0xFFFF;
 constexpr int MAX_CAT_BINS = 256;      // categorical features: <= 256 categories
 constexpr uint32_t UNSAMPLED = 0x80000000u;  // row-list flag: not in the subset
 
-// A feature tile of the histogram: features [f0, f1), whose bins fit in the
+// Layouts of the row-major bin codes that the histogram kernel reads.
+//  TILED: row r holds feature f's code at position f (row stride Fp =
+//         round_up(F, 8)); the code is the entry's index in its feature tile's
+//         shared-memory partial, which holds the tile's bins in global order.
+//  LANES: each tile gives each of the 32 lanes of a warp `slots` code
+//         positions (row stride Fp = tiles * 32 * slots); lane l owns the
+//         features placed in its slots, and the code is the entry's index e
+//         in lane l's own column of the partial, stored at word e * 32 + l,
+//         so the 32 lanes of a warp always add into 32 different banks.
+enum { HIST_LAYOUT_TILED = 0, HIST_LAYOUT_LANES = 1 };
+
+// A feature tile of the histogram: features [f0, f1), whose entries fit in the
 // shared-memory partial of one CTA.
 struct FeatureTile {
   int f0, f1;
   int bin0;       // foff[f0]
   int nbins;      // foff[f1] - foff[f0]
+  int E;          // LANES: entries per lane (the partial has 32 * E words per plane)
+  int ent_off;    // LANES: offset of the tile's (entry, lane) -> histogram-bin table
+  int slot_off;   // LANES: position of the tile's first code in a row
+  int reserved;
 };
 
 struct Ghist {  // sb_ghist
   sb_ctx* ctx = nullptr;
-  size_t n = 0, F = 0, Fp = 0;   // Fp: padded row stride in u16
+  size_t n = 0, F = 0, Fp = 0;   // Fp: row stride of `bins` in u16
   size_t total_bins = 0;
   int max_bin = 0;
   float missing = NAN;
   int max_feature_bins = 0;
   int has_categorical = 0;
-  // [n][Fp] bin codes, tile-relative: code = fbase[f] + local bin, or
-  // fmiss[f] for a missing entry. A code is the entry's index into the
-  // shared-memory partial of the feature's histogram tile.
+  int layout = HIST_LAYOUT_TILED;  // HIST_LAYOUT_*
+  int slots = 0;                   // LANES: code positions per lane and tile
+  // [n][Fp] bin codes of the histogram kernel: feature f of row r at
+  // r * Fp + rpos[f], code = rbase[f] + local bin, or rmiss[f] for a missing
+  // entry; unused positions hold 0xFFFF.
   DBuf<uint16_t> bins;
-  DBuf<uint16_t> bins_col; // [F][n] the same codes, feature-major (partition reads)
-  DBuf<int> fbase;         // [F] foff[f] - tile.bin0
-  DBuf<int> fmiss;         // [F] tile.nbins + (f - tile.f0)
-  std::vector<int> h_fbase, h_fmiss;
+  std::vector<int> h_rpos, h_rbase, h_rmiss;
+  DBuf<int> ent_gbin;      // LANES: per tile, [E][32] histogram bin of each (entry, lane), -1 unused
+  DBuf<int> slot_feat;     // LANES: [Fp] feature of each code position, -1 unused
+  // [F][n] local bins, feature-major, MISSING_BIN for a missing entry (the
+  // partition reads them): code = fbase[f] + local, fmiss[f] when missing
+  DBuf<uint16_t> bins_col;
+  DBuf<int> fbase;         // [F] 0
+  DBuf<int> fmiss;         // [F] MISSING_BIN
   DBuf<uint32_t> foff;     // [F+1]
   DBuf<float> cuts;        // [total_bins]
   DBuf<uint8_t> is_cat;    // [F]
@@ -144,11 +165,31 @@ struct Ghist {  // sb_ghist
   std::vector<float> h_cuts;
   std::vector<uint8_t> h_is_cat;
   std::vector<FeatureTile> tiles;  // histogram feature tiles
-  size_t hist_smem_bytes = 0;      // max tile bytes (8 B per bin)
+  size_t hist_smem_bytes = 0;      // shared memory of the largest tile
 };
+
+// A binned matrix lives on the device of the context that built it; an entry
+// point given a context of another device rejects it before any launch.
+#define SB_SAME_DEVICE(ctx, g)                                                              \
+  SB_REQUIRE((g)->ctx && (g)->ctx->device == (ctx)->device, SB_ERR_INVALID_ARG,            \
+             "the binned matrix is on device %d, the context on device %d",                 \
+             (g)->ctx ? (g)->ctx->device : -1, (ctx)->device)
 
 int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t* h_ftypes,
                 float missing, int max_bin, Ghist* g);
+// The index's device cuts, histogram layout and bin codes from its host cuts
+// (h_foff, h_cuts, h_is_cat; n, F, missing and max_bin set).
+int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g);
+
+// tree_method=approx (sb_approx.cu): a matrix's columns sorted once, then
+// hessian-weighted cuts (HistCuts::from_dmatrix_weighted) for any hessians.
+struct ApproxState;
+ApproxState* approx_state_new();
+void approx_state_free(ApproxState* a);
+int approx_prepare(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t* h_ftypes, float missing,
+                   int max_bin, ApproxState* A);
+// host cuts into g (h_foff, h_cuts, h_is_cat) for device hessians d_hess[n] >= 0
+int approx_cuts(ApproxState* A, const float* d_hess, Ghist* g);
 
 // ------------------------------------------------------------ histograms
 // One node histogram to accumulate: rows[begin..end) of a row list.
@@ -217,6 +258,10 @@ struct DevEnsemble {
   DBuf<int> chunk_fo;        // [n_shap_chunks + 1] offsets into chunk_f
   DBuf<int> chunk_f;         // the distinct features of each chunk's paths
   int shap_max_fc = 1;       // most distinct features in one chunk
+  bool shap_valid = false;   // the TreeSHAP state above has been built (shap_prepare)
+  bool shap_table = false;   // per-path contribution tables are in use
+  DBuf<float> shap_tab;      // per path: [2^D][round_up(D, 4)] f32 contributions
+  DBuf<long long> shap_tab_off;  // [n_paths] first float of each path's table
   int n_trees = 0;
   int max_depth = 0;
   int max_path_len = 0;      // elements, bias included
@@ -243,6 +288,13 @@ namespace sb {
 
 int n_outputs(int objective, int num_class);
 int model_upload(sb_model* m);
+int tree_depth(const HostTree& t);
+double node_mean_value(const HostTree& t, int id);  // learner/shap.rs:288-302
+// TreeSHAP (sb_shap.cu): the model's path data and tables, built once
+int shap_prepare(sb_model* m);
+int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing, float* d_out);
+int predict_interactions_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing,
+                                float* d_out);
 
 // The trees a booster has grown so far, as they sit on the device: tree
 // t = round * K + class at nodes[t * maxn ..], its categories at

@@ -61,6 +61,7 @@ int sb_hist_build_static(sb_ctx* ctx, const sb_ghist* g, const uint32_t* d_rows,
                          const sb_gradpair* d_gpair, size_t n, sb_gradstats* d_out, size_t total_bins) {
   using namespace sb;
   SB_REQUIRE(ctx && g && d_gpair && d_out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_SAME_DEVICE(ctx, g);
   SB_REQUIRE(m == 0 || d_rows, SB_ERR_INVALID_ARG, "d_rows is NULL");
   SB_REQUIRE(total_bins == g->total_bins, SB_ERR_DIMENSION,
              "dimension mismatch: out length expected %zu, got %zu", g->total_bins, total_bins);

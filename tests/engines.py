@@ -104,7 +104,9 @@ class GpuEngine:
         return m.predict_margin(self.sb.DMatrix(x))
 
     def gradient(self, obj, preds, labels, weights, k, spw):
-        raise NotImplementedError
+        w = None if weights is None else np.asarray(weights, np.float32)
+        return self.sb.objective_gradient(obj, preds, labels, w, num_class=k, scale_pos_weight=spw,
+                                          ctx=self.ctx)
 
     def train(self, x, y, p, rounds, base_margin=None, ftypes=None, want_contribs=False,
               want_interactions=False):

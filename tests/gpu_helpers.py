@@ -1,5 +1,31 @@
 """Helpers shared by the GPU parity tests."""
+import contextlib
+import os
+
 import numpy as np
+
+# The histogram's bin-code layouts: "tiled" (a feature's bins contiguous in
+# shared memory) and "lanes" (each lane of a warp owns its features' bins in
+# its own bank). An index picks one by shape; SB_HIST_LAYOUT forces one for
+# the indexes built while it is set.
+LAYOUTS = ["tiled", "lanes"]
+
+
+@contextlib.contextmanager
+def hist_layout(name):
+    """Indexes built inside the block use the given layout (None: by shape)."""
+    old = os.environ.get("SB_HIST_LAYOUT")
+    if name is None:
+        os.environ.pop("SB_HIST_LAYOUT", None)
+    else:
+        os.environ["SB_HIST_LAYOUT"] = name
+    try:
+        yield
+    finally:
+        if old is None:
+            os.environ.pop("SB_HIST_LAYOUT", None)
+        else:
+            os.environ["SB_HIST_LAYOUT"] = old
 
 
 def mixed_data(n, f=12, seed=0, nan_frac=0.1, n_cat=0, card=8):

@@ -65,3 +65,24 @@ def test_dart_multiclass_learns(sb, ctx):
     assert np.mean(np.argmax(pr, axis=1) == y) > 0.9
     with pytest.raises(sb.SbError):
         sb.train_with_eval(p, sb.DMatrix(x, labels=y), 2, [(sb.DMatrix(x, labels=y), "t")], ctx=ctx)
+
+
+@pytest.mark.parametrize("objective", ["reg:squarederror", "reg:pseudohubererror"])
+def test_dart_matches_the_oracle_restatement(sb, ctx, orc, objective):
+    """dart_round (train.rs:384-456) against the oracle's restatement with the
+    same dropout stream: the trees, their weights (1/(k+1) for new trees,
+    k/(k+1) for dropped ones) and the margins equal the oracle's bit for bit
+    on the default fixed-point form."""
+    x, _ = mixed_data(6000, 8, seed=71)
+    rng = np.random.default_rng(72)
+    y = (np.sin(np.nan_to_num(x[:, 0])) + np.nan_to_num(x[:, 1]) + 0.1 * rng.standard_normal(len(x))).astype(np.float32)
+    p = sb.TrainingParams(objective=objective, booster="dart", rate_drop=0.3, skip_drop=0.1, max_depth=4, eta=0.3,
+                          subsample=0.8, seed=13)
+    m = sb.train(p, sb.DMatrix(x, labels=y), 10, ctx=ctx)
+    ref = orc.train_dart(x, y, p, 10)
+    got, want = m.export(), ref["model"].export()
+    from gpu_helpers import assert_trees_equal
+    assert_trees_equal(got, want)
+    assert np.array_equal(got[4], want[4])
+    assert np.any(got[4] < 1.0)
+    assert np.array_equal(m.predict_margin(sb.DMatrix(x)), ref["margins"].reshape(-1))

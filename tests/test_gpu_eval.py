@@ -122,8 +122,9 @@ def test_eval_history_and_metric_errors(sb, ctx):
     y = np.nan_to_num(x[:, 0]).astype(np.float32)
     d = sb.DMatrix(x, labels=y)
     dv = sb.DMatrix(x[:500], labels=y[:500])
-    # fixed point: the histograms, and so the trees, do not depend on atomic order
-    p = sb.TrainingParams(objective="reg:squarederror", max_depth=4, hist_precision="fixed")
+    # default precision (fixed point): the histograms, and so the trees, do not
+    # depend on the order of atomic additions, so two trainings are equal
+    p = sb.TrainingParams(objective="reg:squarederror", max_depth=4)
     res = sb.train_with_eval(p, d, 12, [(d, "train"), (dv, "valid")], ctx=ctx)
     assert len(res.history) == 12 and res.model.num_trees() == 12
     assert [s[:2] for s in res.history[0].scores] == [("train", "rmse"), ("valid", "rmse")]

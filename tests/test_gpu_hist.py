@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from engines import GpuEngine
-from gpu_helpers import mixed_data, random_gpair
+from gpu_helpers import LAYOUTS, hist_layout, mixed_data, random_gpair
 from kat_checks import check_case
 
 pytestmark = pytest.mark.gpu
@@ -21,13 +21,15 @@ def test_hist_reference_kats(case, sb, ctx):
     check_case(case, GpuEngine(sb, ctx), sb.TrainingParams)
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("n,f,frac", [(2000, 10, 1.0), (60000, 40, 0.7), (200000, 100, 0.5)])
-def test_fp32_within_1e5_of_f64(sb, ctx, orc, n, f, frac):
+def test_fp32_within_1e5_of_f64(sb, ctx, orc, n, f, frac, layout):
     x, _ = mixed_data(n, f, seed=n)
     g = random_gpair(n, seed=1, logistic=True)
     rng = np.random.default_rng(2)
     rows = np.sort(rng.choice(n, int(n * frac), replace=False)).astype(np.uint32)
-    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    with hist_layout(layout):
+        gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
     got = sb.GpuBackend("fp32", ctx=ctx).build(gh, rows, g)
     d = orc.data(x)
     want = d.hist(rows, g, threads=8)
@@ -38,15 +40,17 @@ def test_fp32_within_1e5_of_f64(sb, ctx, orc, n, f, frac):
     assert np.all(err <= 1e-5 * mag + 1e-12), float(np.max(err / (mag + 1e-30)))
 
 
-@pytest.mark.parametrize("bits", [12, 16, 20])
-def test_fixed_point_is_exact(sb, ctx, orc, bits):
-    n, f = 100000, 30
+@pytest.mark.parametrize("layout", LAYOUTS)
+@pytest.mark.parametrize("bits,f", [(12, 30), (16, 30), (20, 30), (16, 50), (16, 100)])
+def test_fixed_point_is_exact(sb, ctx, orc, bits, f, layout):
+    n = 100000
     x, _ = mixed_data(n, f, seed=7, n_cat=2, card=16)
     ft = np.zeros(f, np.uint8)
     ft[-2:] = 1
     g = random_gpair(n, seed=3)
     rows = np.arange(0, n, 3, dtype=np.uint32)
-    gh = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx)
+    with hist_layout(layout):
+        gh = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx)
     got = sb.GpuBackend("fixed", quantize_bits=bits, ctx=ctx).build(gh, rows, g)
     gq, _, _ = orc.quantize(g, bits)
     want = orc.data(x, ft).hist(rows, gq, threads=1)
@@ -68,3 +72,15 @@ def test_dimension_mismatch_is_reported(sb, ctx):
     gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
     with pytest.raises(sb.SbError):
         sb.GpuBackend(ctx=ctx).build(gh, np.arange(10, dtype=np.uint32), random_gpair(99))
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_local_bins_do_not_depend_on_layout(sb, ctx, layout):
+    """The exported local bins (GHistIndex::bins) are the same whichever
+    layout the histogram kernel reads."""
+    x, ft = mixed_data(5000, 37, seed=4, n_cat=3, card=9)
+    with hist_layout(None):
+        ref = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx).local_bins()
+    with hist_layout(layout):
+        got = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx).local_bins()
+    assert np.array_equal(got, ref)

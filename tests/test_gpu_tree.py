@@ -8,12 +8,13 @@ the row-to-leaf assignment. FP32 form: structure must match wherever the
 oracle's best-vs-runner-up gain gap exceeds the tolerance."""
 import json
 import os
+import zlib
 
 import numpy as np
 import pytest
 
 from engines import GpuEngine
-from gpu_helpers import assert_trees_equal, leaf_ids, mixed_data, random_gpair
+from gpu_helpers import LAYOUTS, assert_trees_equal, hist_layout, leaf_ids, mixed_data, random_gpair
 from kat_checks import check_case
 
 pytestmark = pytest.mark.gpu
@@ -39,16 +40,18 @@ VARIANTS = {
 }
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("logistic", [False, True])
-def test_fixed_point_tree_bit_exact(sb, ctx, orc, variant, logistic):
+def test_fixed_point_tree_bit_exact(sb, ctx, orc, variant, logistic, layout):
     n, f = 40000, 12
-    x, _ = mixed_data(n, f, seed=hash(variant) % 1000)
+    x, _ = mixed_data(n, f, seed=zlib.crc32(variant.encode()) % 1000)
     g = random_gpair(n, seed=5, logistic=logistic)
     rng = np.random.default_rng(6)
     rows = np.sort(rng.choice(n, int(n * 0.8), replace=False)).astype(np.uint32)
     p = sb.TrainingParams(hist_precision="fixed", **VARIANTS[variant])
-    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    with hist_layout(layout):
+        gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
     m, row_leaf = sb.HistTreeBuilder(p, ctx=ctx).build(gh, g, rows, round=3, return_row_leaf=True)
     gq, _, _ = orc.quantize(g, 16)
     om = orc.tree_build(orc.data(x), p, gq, rows, round_=3)
@@ -63,13 +66,15 @@ def test_fixed_point_tree_bit_exact(sb, ctx, orc, variant, logistic):
     assert np.all(row_leaf[~in_subset] == -1)
 
 
-def test_fixed_point_categorical_tree_bit_exact(sb, ctx, orc):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_fixed_point_categorical_tree_bit_exact(sb, ctx, orc, layout):
     n, f = 30000, 10
     x, ft = mixed_data(n, f, seed=21, n_cat=3, card=24)
     g = random_gpair(n, seed=8)
     rows = np.arange(n, dtype=np.uint32)
     p = sb.TrainingParams(hist_precision="fixed", max_depth=6)
-    gh = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx)
+    with hist_layout(layout):
+        gh = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx)
     m = sb.HistTreeBuilder(p, ctx=ctx).build(gh, g, rows)
     gq, _, _ = orc.quantize(g, 16)
     om = orc.tree_build(orc.data(x, ft), p, gq, rows)

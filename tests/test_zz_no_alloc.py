@@ -17,7 +17,7 @@ def _static_build(sb, ctx, gh, d_rows, m, d_gpair, n, d_out, total):
                                     ctypes.c_void_p(d_out), total)
 
 
-def test_static_scratch_build_matches_sb_hist_build_twice(sb, ctx):
+def test_static_scratch_build_matches_sb_hist_build_twice(sb, ctx, orc):
     import torch
     n, f = 60000, 24
     x, _ = mixed_data(n, f, seed=11)
@@ -43,6 +43,10 @@ def test_static_scratch_build_matches_sb_hist_build_twice(sb, ctx):
         # a different order: equal within 1e-5 of each bin's absolute mass
         mag = sb.GpuBackend("fp32", ctx=ctx).build(gh, rows, np.abs(g))
         err = np.abs(got - want)
+        assert np.all(err <= 1e-5 * mag + 1e-12), (call, float(np.max(err / (mag + 1e-30))))
+        # and against the oracle's f64 CpuBackend::build on the same rows
+        ref = orc.data(x).hist(rows, g)
+        err = np.abs(got - ref)
         assert np.all(err <= 1e-5 * mag + 1e-12), (call, float(np.max(err / (mag + 1e-30))))
 
 
@@ -74,3 +78,32 @@ def test_static_scratch_rejects_bad_rows_and_large_indexes(sb, ctx):
     rc = _static_build(sb, ctx, gb, d_rb.data_ptr(), 300, d_gb.data_ptr(), 300, d_ob.data_ptr(), tb)
     assert rc == sb._abi.SB_ERR_UNSUPPORTED
     assert b"SB_STATIC_SCRATCH_BYTES" in sb._abi.lib().sb_last_error()
+
+
+def test_static_scratch_through_a_second_context(sb, ctx, orc):
+    """A second context on the same device reuses the scratch address the
+    first context's calls looked up; its results match sb_hist_build and the
+    oracle."""
+    import torch
+    n, f = 30000, 16
+    x, _ = mixed_data(n, f, seed=14)
+    ctx2 = sb.Context(0)
+    gh2 = sb.GHistIndex(sb.DMatrix(x), ctx=ctx2)
+    total = gh2.total_bins
+    g = random_gpair(n, seed=33)
+    rows = np.arange(1, n, 2, dtype=np.uint32)
+    dev = torch.device("cuda", 0)
+    d_rows = torch.from_numpy(rows.astype(np.int32)).to(dev)
+    d_g = torch.from_numpy(np.ascontiguousarray(g, np.float32)).to(dev)
+    want = sb.GpuBackend("fp32", ctx=ctx2).build(gh2, rows, g)
+    mag = sb.GpuBackend("fp32", ctx=ctx2).build(gh2, rows, np.abs(g))
+    ref = orc.data(x).hist(rows, g)
+    for _ in range(2):
+        d_out = torch.full((total, 2), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        rc = _static_build(sb, ctx2, gh2, d_rows.data_ptr(), rows.size, d_g.data_ptr(), n, d_out.data_ptr(),
+                           total)
+        assert rc == 0, sb._abi.lib().sb_last_error()
+        got = d_out.cpu().numpy()
+        assert np.all(np.abs(got - want) <= 1e-5 * mag + 1e-12)
+        assert np.all(np.abs(got - ref) <= 1e-5 * mag + 1e-12)
