@@ -56,6 +56,11 @@ def parse():
     ap.add_argument("--cpu-rounds", type=int, default=20)
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-c0", action="store_true")
+    ap.add_argument("--no-c2", action="store_true")
+    ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--c2-rows", type=int, default=2_000_000)
+    ap.add_argument("--c2-rounds", type=int, default=5)
+    ap.add_argument("--c3-jobs", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
@@ -347,6 +352,68 @@ def serving_leg(sb, ctx, args, torch):
             "prediction": pred}
 
 
+def c2_leg(sb, ctx, args, torch):
+    """The multiclass lossguide workload: multiclass_uniform 2M x 200 (U(0,1),
+    features 195-199 categorical with 32 codes), 10 classes, multi:softprob,
+    lossguide with max_leaves 255 and max_depth 0, max_bin 256, monotone +1 on
+    feature 0 and -1 on feature 1; all 10 class trees of a round grow in the
+    same launches. A step is one round (10 trees); CUDA events on the
+    library's stream."""
+    from sequoia_boost_b200 import datagen
+    n = args.c2_rows
+    x, y, ft = datagen.multiclass_uniform(n=n, seed=args.seed + 2)
+    xd = torch.from_numpy(x).to(f"cuda:{ctx.device}")
+    gh = sb.GHistIndex.from_device(xd.data_ptr(), n, x.shape[1], max_bin=256, feature_types=ft, ctx=ctx)
+    del xd
+    p = sb.TrainingParams(objective="multi:softprob", num_class=10, grow_policy="lossguide", max_leaves=255,
+                          max_depth=0, max_bin=256, eta=0.3, monotone_constraints=[1, -1], seed=7)
+    b = sb.Booster(gh, p, y, ctx=ctx)
+    b.update(2)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    e0.record(stream)
+    b.update(args.c2_rounds)
+    e1.record(stream)
+    ctx.synchronize()
+    ms = e0.elapsed_time(e1)
+    b.set_timing(True)
+    b.reset_stats()
+    b.update(1)
+    st = b.stats()
+    m = b.margins().reshape(n, 10).astype(np.float64)
+    m -= m.max(axis=1, keepdims=True)
+    lp = m - np.log(np.exp(m).sum(axis=1, keepdims=True))
+    mll = float(-np.mean(lp[np.arange(n), y.astype(np.int64)]))
+    out = {"workload": f"multiclass_uniform {n} x 200, 10 classes, lossguide max_leaves 255, 5 categorical, "
+                       "monotone on features 0 and 1", "value": n * args.c2_rounds / (ms / 1e3) / 1e6,
+           "unit": UNIT, "ms_per_round": ms / args.c2_rounds, "rounds_timed": args.c2_rounds,
+           "hist_ms_per_launch": st["hist_ms"] / max(st["hist_launches"], 1),
+           "hist_launches_per_round": st["hist_launches"], "train_mlogloss": mll}
+    del b, gh
+    return out
+
+
+def c3_leg(sb, ctx, args):
+    """256 independent regression jobs (small_jobs: rows log-uniform in [1k,
+    200k], 20-50 N(0,1) features, max_depth in {4,6,8}, eta in {0.05, 0.1,
+    0.3}, 100 rounds, max_bin 64) trained together by one sb_train_many call
+    from host buffers (upload, binning, rounds, model download)."""
+    from sequoia_boost_b200 import datagen
+    jobs = datagen.small_jobs(n_jobs=args.c3_jobs, seed=args.seed + 3)
+    spec = [(sb.TrainingParams(objective="reg:squarederror", max_depth=j["max_depth"], eta=j["eta"], max_bin=64),
+             sb.DMatrix(j["x"], labels=j["y"]), 100) for j in jobs]
+    sb.train_many(spec[:4], ctx=ctx)  # warm-up
+    t0 = time.perf_counter()
+    models = sb.train_many(spec, n_streams=16, ctx=ctx)
+    t = time.perf_counter() - t0
+    rows = sum(j["x"].shape[0] for j in jobs)
+    assert all(m is not None for m in models)
+    return {"workload": f"{len(jobs)} regression jobs, {rows} rows in total, 20-50 features, 100 rounds each, "
+                        "max_bin 64, one sb_train_many call (16 streams)",
+            "value": rows * 100 / t / 1e6, "unit": UNIT, "seconds": t}
+
+
 def run_reference(args):
     """The reference arm: the reference's CPU hist path (oracle port), all host
     threads, a bounded sample of the same workload per step."""
@@ -531,6 +598,8 @@ def main():
     serving = None
     if not args.no_serve and rank == 0:
         serving = serving_leg(sb, ctx, args, torch)
+    c2 = c2_leg(sb, ctx, args, torch) if not args.no_c2 and rank == 0 else None
+    c3 = c3_leg(sb, ctx, args) if not args.no_c3 and rank == 0 else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -538,7 +607,8 @@ def main():
                 "dtype": "i64" if args.precision == "fixed" else "f32", "data": "synthetic",
                 "config": config_of(args, n), "clocks": clk, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "quality": quality,
-                "fp32_arm": fp32, "matched_quality": matched, "c0": c0, "serving": serving}
+                "fp32_arm": fp32, "matched_quality": matched, "c0": c0, "c2": c2, "c3": c3,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -14,6 +14,11 @@
 // passes over X give exact values, identical to the sorted-array reads.
 #include <cstring>
 
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "sb_internal.cuh"
 
 namespace sb {
@@ -413,6 +418,27 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
 
 }  // namespace
 
+namespace {
+
+// Indexes with fewer rows take the default layout without timing.
+constexpr size_t TUNE_MIN_ROWS = 200000;
+
+// Shape bucket of the autotuner: device, features, most bins of a feature,
+// log2 of the rows, categorical features present.
+struct TuneKey {
+  int device, F, max_bins, log2_rows, categorical;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, F, max_bins, log2_rows, categorical) <
+           std::tie(o.device, o.F, o.max_bins, o.log2_rows, o.categorical);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, HistChoice> g_tuned;
+
+}  // namespace
+
+int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g);
+
 int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t* h_ftypes,
                 float missing, int max_bin, Ghist* g) {
   SB_REQUIRE(n > 0 && F > 0, SB_ERR_INVALID_ARG, "empty dataset: zero rows or columns");
@@ -519,7 +545,6 @@ int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t
 // copies of the cuts, the histogram layout and the bin codes of every entry.
 int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
   const size_t n = g->n, F = g->F;
-  const float missing = g->missing;
   cudaStream_t st = ctx->stream;
   g->total_bins = g->h_cuts.size();
   g->max_feature_bins = 0;
@@ -537,7 +562,58 @@ int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_CUDA(cudaMemcpyAsync(g->foff.p, g->h_foff.data(), (F + 1) * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(g->cuts.p, g->h_cuts.data(), g->total_bins * 4, cudaMemcpyHostToDevice, st));
 
-  SB_TRY(hist_prepare(ctx, g));  // the histogram layout fixes the row codes
+  // the histogram layout fixes the row codes: the default choice, or the
+  // fastest candidate for this shape (timed once per shape and device)
+  HistChoice choice;
+  SB_TRY(hist_default_choice(ctx, g, &choice));
+  const char* at = std::getenv("SB_HIST_AUTOTUNE");
+  const bool tune = !std::getenv("SB_HIST_LAYOUT") && !(at && std::strcmp(at, "0") == 0) && n >= TUNE_MIN_ROWS;
+  if (tune) {
+    int lg = 0;
+    while ((size_t(2) << lg) <= n) ++lg;
+    const TuneKey key{ctx->device, (int)F, g->max_feature_bins, lg, g->has_categorical};
+    bool cached = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) {
+        choice = it->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      const std::vector<HistChoice> cands = hist_candidates(ctx, g);
+      float best_t = 1e30f;
+      HistChoice best = choice, last{-1, -1};
+      for (const HistChoice& c : cands) {
+        SB_TRY(hist_prepare(ctx, g, c));
+        SB_TRY(bin_codes(ctx, d_X, g));
+        float t = 0.0f;
+        SB_TRY(hist_time(ctx, g, &t));
+        last = c;
+        if (t < best_t) {
+          best_t = t;
+          best = c;
+        }
+      }
+      {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[key] = best;
+      }
+      if (best.layout == last.layout && best.slots == last.slots) return SB_OK;  // built already
+      choice = best;
+    }
+  }
+  SB_TRY(hist_prepare(ctx, g, choice));
+  return bin_codes(ctx, d_X, g);
+}
+
+// The bin codes of every entry for the planned layout (and the feature-major
+// local bins).
+int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
+  const size_t n = g->n, F = g->F;
+  const float missing = g->missing;
+  cudaStream_t st = ctx->stream;
   // feature-major codes are the local bins themselves
   const std::vector<int> zeros(F, 0), miss(F, (int)MISSING_BIN);
   SB_TRY(g->fbase.alloc(ctx, F));

@@ -3,20 +3,26 @@
 // Replaces CpuBackend::build / accumulate (tree/hist/mod.rs:58-119) and
 // `subtracted` / HistogramBackend::subtract (:25-28, :38-44).
 //
-// Design: a persistent grid (one or more CTAs per SM) splits the concatenated
-// rows of every node to build (all frontier nodes of all class trees in one
-// launch) evenly over CTAs. A CTA keeps one node's histogram for one feature
-// tile in shared memory, walks the node's row list with one warp per row and
-// one lane per feature (coalesced 64-byte reads of the row's u16 bins), adds
-// into shared memory, and flushes non-zero bins to the node's HBM histogram
-// with global atomics when it moves to the next node.
-//   FP32 form : two f32 shared atomics per entry; HBM histograms in f64.
-//   FIXED form: gradients pre-rounded to |q| <= 2^bits with a per-round
-//               power-of-two scale and packed as (q_g << 32) + q_h; one 64-bit
-//               integer shared atomic per entry accumulates both halves
-//               exactly (carries cannot cross: sum q_h < 2^32 and
-//               |sum q_g| < 2^31 are kept by flushing every
-//               fixed_rows_per_flush(bits) rows); HBM histograms in int64.
+// Design: a persistent grid (one CTA of 1024 threads per SM) splits the
+// concatenated rows of every node to build (all frontier nodes of all class
+// trees in one launch) evenly over CTAs. A CTA keeps one node's histogram for
+// one feature tile in shared memory, walks its rows eight per warp (lanes 0-7
+// load the row ids one batch ahead and the gradient pairs, shuffles hand them
+// to the warp), adds every code of a row into the shared partial, and flushes
+// the non-zero entries to the node's HBM histogram with global atomics when it
+// moves to the next piece.
+//   codes  TILED layout: lane l reads features 4l..4l+3 of the tile (one
+//          8-byte load per row) and a code is the entry's index in the tile's
+//          partial, where a feature's bins are contiguous. LANES layout: each
+//          tile gives lane l `S` (1, 2 or 4) code positions of the row, packed
+//          with features so that every lane's entries fit its own column, and
+//          entry e of lane l sits at word e * 32 + l: the 32 lanes of a warp
+//          always add into 32 different banks.
+//   sums   FP32 form: f32 shared atomics, f64 node histograms. FIXED form:
+//          gradients rounded to |q| <= 2^bits with a per-round power-of-two
+//          scale; one int32 and one uint32 shared atomic per entry, exact
+//          because a CTA flushes at least every fixed_rows_per_flush(bits)
+//          rows; int64 node histograms (order independent).
 // Each feature also owns one extra "missing" bin (index total_bins + f), so a
 // node's missing-value statistics are summed directly instead of being
 // recovered as total - present.
@@ -576,29 +582,29 @@ size_t lanes_smem(const Ghist* g) {
 
 }  // namespace
 
-// Chooses the layout of the histogram's bin codes and its feature tiles. The
-// LANES layout (conflict-free shared atomics) is taken when every feature
-// fits one lane's column and its rows are at most 1.3x the TILED rows (its
-// rows hold 32 lanes x `slots` positions per tile, padded); SB_HIST_LAYOUT
-// = "tiled" or "lanes" in the environment forces one (for measurements).
-int hist_prepare(sb_ctx* ctx, Ghist* g) {
-  const size_t budget = ctx->smem_optin > 8192 ? ctx->smem_optin - 4096 : ctx->smem_optin;
+namespace {
+
+size_t smem_budget(const sb_ctx* ctx) {
+  return ctx->smem_optin > 8192 ? ctx->smem_optin - 4096 : ctx->smem_optin;
+}
+
+}  // namespace
+
+// Plans the histogram's bin-code layout and feature tiles for one choice
+// (HIST_LAYOUT_TILED, or HIST_LAYOUT_LANES with 1, 2 or 4 code positions per
+// lane and tile). SB_ERR_UNSUPPORTED when a feature's entries do not fit one
+// lane's column.
+int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
+  const size_t budget = smem_budget(ctx);
   const size_t F = g->F;
-  const char* force = std::getenv("SB_HIST_LAYOUT");
-  const bool force_tiled = force && std::strcmp(force, "tiled") == 0;
-  const bool force_lanes = force && std::strcmp(force, "lanes") == 0;
-  const int slots = F <= 32 ? 1 : (F <= 64 ? 2 : 4);
-  std::vector<std::vector<LanePlace>> places;
-  bool lanes = false;
-  if (!force_tiled && plan_lanes(g, budget, slots, &places) == SB_OK) {
-    const size_t lanes_row = g->tiles.size() * 32 * slots;
-    const size_t tiled_row = (F + 7) / 8 * 8;
-    lanes = force_lanes || lanes_row * 10 <= tiled_row * 13;
-  }
-  SB_REQUIRE(!force_lanes || lanes, SB_ERR_UNSUPPORTED, "SB_HIST_LAYOUT=lanes: a feature has too many bins");
-  if (!lanes) {
+  if (c.layout == HIST_LAYOUT_TILED) {
     SB_TRY(plan_tiled(g, budget));
   } else {
+    const int slots = c.slots;
+    SB_REQUIRE(slots == 1 || slots == 2 || slots == 4, SB_ERR_INVALID_ARG, "internal: %d slots", slots);
+    std::vector<std::vector<LanePlace>> places;
+    SB_REQUIRE(plan_lanes(g, budget, slots, &places) == SB_OK, SB_ERR_UNSUPPORTED,
+               "a feature has too many bins for the lane layout");
     g->layout = HIST_LAYOUT_LANES;
     g->slots = slots;
     g->Fp = g->tiles.size() * 32 * slots;
@@ -638,6 +644,39 @@ int hist_prepare(sb_ctx* ctx, Ghist* g) {
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 4>, g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 4>, g->hist_smem_bytes));
   return SB_OK;
+}
+
+// The layout an index takes without timing: TILED, or what SB_HIST_LAYOUT
+// ("tiled" or "lanes") in the environment forces. On the 10M x 100 binary
+// workload TILED measured 0.41 ms per histogram launch against 0.48 ms for
+// LANES with 4 positions per lane, so LANES is only chosen by timing.
+int hist_default_choice(sb_ctx* ctx, Ghist* g, HistChoice* out) {
+  const size_t F = g->F;
+  const char* force = std::getenv("SB_HIST_LAYOUT");
+  const bool force_lanes = force && std::strcmp(force, "lanes") == 0;
+  *out = HistChoice{HIST_LAYOUT_TILED, 0};
+  if (!force_lanes) return SB_OK;
+  const int slots = F <= 32 ? 1 : (F <= 64 ? 2 : 4);
+  std::vector<std::vector<LanePlace>> places;
+  const std::vector<FeatureTile> keep = g->tiles;
+  const bool ok = plan_lanes(g, smem_budget(ctx), slots, &places) == SB_OK;
+  g->tiles = keep;
+  SB_REQUIRE(ok, SB_ERR_UNSUPPORTED, "SB_HIST_LAYOUT=lanes: a feature has too many bins");
+  *out = HistChoice{HIST_LAYOUT_LANES, slots};
+  return SB_OK;
+}
+
+// Every choice that fits the index: TILED, and LANES with 1, 2 and 4
+// positions per lane where its features pack.
+std::vector<HistChoice> hist_candidates(sb_ctx* ctx, Ghist* g) {
+  std::vector<HistChoice> out{HistChoice{HIST_LAYOUT_TILED, 0}};
+  const std::vector<FeatureTile> keep = g->tiles;
+  for (int slots : {1, 2, 4}) {
+    std::vector<std::vector<LanePlace>> places;
+    if (plan_lanes(g, smem_budget(ctx), slots, &places) == SB_OK) out.push_back(HistChoice{HIST_LAYOUT_LANES, slots});
+  }
+  g->tiles = keep;
+  return out;
 }
 
 namespace {
@@ -703,6 +742,76 @@ int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const 
   dim3 grid((unsigned)std::min<size_t>((words + 255) / 256, 64), (unsigned)max_items);
   SB_LAUNCH(ctx, k_zero_items, grid, 256, 0, items, count, words);
   return SB_OK;
+}
+
+// Device time of one fixed-point histogram launch over the first min(n,
+// 2^20) rows (all in the row list), best of two after a warm-up launch: the
+// autotuner's measure.
+int hist_time(sb_ctx* ctx, const Ghist* g, float* ms) {
+  const size_t m = std::min<size_t>(g->n, (size_t)1 << 20);
+  const size_t HB = g->total_bins + g->F;
+  cudaStream_t st = ctx->stream;
+  DBuf<uint32_t> rows;
+  DBuf<unsigned long long> gp;
+  DBuf<longlong2> out;
+  DBuf<HistItem> item;
+  DBuf<uint64_t> prefix;
+  DBuf<int> count;
+  DBuf<FeatureTile> tiles;
+  SB_TRY(rows.alloc(ctx, m));
+  SB_TRY(gp.alloc_zero(ctx, g->n));
+  SB_TRY(out.alloc(ctx, HB));
+  SB_TRY(item.alloc(ctx, 1));
+  SB_TRY(prefix.alloc(ctx, 2));
+  SB_TRY(count.alloc(ctx, 1));
+  SB_TRY(tiles.alloc(ctx, g->tiles.size()));
+  std::vector<uint32_t> h_rows(m);
+  for (size_t i = 0; i < m; ++i) h_rows[i] = (uint32_t)i;
+  HistItem it{};
+  it.rows = rows.p;
+  it.begin = 0;
+  it.end = (uint32_t)m;
+  it.out = out.p;
+  const uint64_t h_prefix[2] = {0, (uint64_t)m};
+  const int one = 1;
+  SB_CUDA(cudaMemcpyAsync(rows.p, h_rows.data(), m * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(item.p, &it, sizeof(it), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(prefix.p, h_prefix, sizeof(h_prefix), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(count.p, &one, sizeof(one), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(tiles.p, g->tiles.data(), g->tiles.size() * sizeof(FeatureTile), cudaMemcpyHostToDevice,
+                          st));
+  HistLaunch L;
+  L.g = g;
+  L.gpair = gp.p;
+  L.fixed = 1;
+  L.quant_bits = 16;
+  L.items = item.p;
+  L.prefix = prefix.p;
+  L.count = count.p;
+  L.max_items = 1;
+  L.tiles = tiles.p;
+  L.ntiles = (int)g->tiles.size();
+  L.rows_done = nullptr;
+  L.pool_mask = nullptr;
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int rc = SB_OK;
+  for (int rep = 0; rep < 3 && rc == SB_OK; ++rep) {
+    cudaMemsetAsync(out.p, 0, out.bytes(), st);
+    cudaEventRecord(e0, st);
+    rc = launch_hist(ctx, L);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = SB_ERR_CUDA;
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (rep > 0) best = std::min(best, t);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = best;
+  return rc;
 }
 
 // per-node seam helpers (defined in sb_grow.cu)

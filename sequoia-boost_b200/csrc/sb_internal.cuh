@@ -217,7 +217,16 @@ struct HistLaunch {
   const uint32_t* pool_mask;      // device [K][ceil(F/32)]: features to accumulate, or null
 };
 
-int hist_prepare(sb_ctx* ctx, Ghist* g);
+// One layout of the histogram's bin codes (HIST_LAYOUT_*; LANES: positions
+// per lane and tile, 1, 2 or 4).
+struct HistChoice {
+  int layout;
+  int slots;
+};
+int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c);
+int hist_default_choice(sb_ctx* ctx, Ghist* g, HistChoice* out);
+std::vector<HistChoice> hist_candidates(sb_ctx* ctx, Ghist* g);
+int hist_time(sb_ctx* ctx, const Ghist* g, float* ms);
 int launch_hist(sb_ctx* ctx, const HistLaunch& L);
 int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const int* count,
                       int max_items);

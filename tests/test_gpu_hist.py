@@ -84,3 +84,19 @@ def test_local_bins_do_not_depend_on_layout(sb, ctx, layout):
     with hist_layout(layout):
         got = sb.GHistIndex(sb.DMatrix(x, feature_types=ft), ctx=ctx).local_bins()
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("f", [24, 60, 100])
+def test_autotuned_index_is_exact(sb, ctx, orc, f):
+    """Indexes of 200k rows and more time every layout that fits their shape
+    (TILED, LANES with 1, 2 or 4 positions per lane) on one histogram launch
+    and keep the fastest; whichever wins, the histograms are exact."""
+    n = 250_000
+    x, _ = mixed_data(n, f, seed=f)
+    g = random_gpair(n, seed=f + 1)
+    rows = np.arange(1, n, 2, dtype=np.uint32)
+    with hist_layout(None):
+        gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    got = sb.GpuBackend("fixed", quantize_bits=16, ctx=ctx).build(gh, rows, g)
+    gq, _, _ = orc.quantize(g, 16)
+    assert np.array_equal(got, orc.data(x).hist(rows, gq, threads=8))
