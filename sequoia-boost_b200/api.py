@@ -601,13 +601,17 @@ def objective_gradient(objective, preds, labels, weights=None, num_class=0, scal
     `preds` [n][K] -> GradPair [n][K] as an (n*K, 2) f32 array, with the code
     the boosting rounds use (sb_objective_gradient)."""
     ctx = ctx or default_context()
-    if objective not in OBJECTIVES:
+    if isinstance(objective, (int, np.integer)):
+        code = int(objective)  # an SB_OBJ_* code
+    elif objective in OBJECTIVES:
+        code = OBJECTIVES[objective]
+    else:
         raise A.SbError(A.SB_ERR_INVALID_ARG, f"unknown value `{objective}` for objective")
     preds = _f32(preds).reshape(-1)
     labels = _f32(labels).reshape(-1)
     w = None if weights is None else _f32(weights).reshape(-1)
     out = np.zeros((preds.size, 2), np.float32)
-    A.check(A.lib().sb_objective_gradient(ctx.h, OBJECTIVES[objective], num_class, float(scale_pos_weight),
+    A.check(A.lib().sb_objective_gradient(ctx.h, code, num_class, float(scale_pos_weight),
                                           A.ptr(preds, ctypes.c_float), A.ptr(labels, ctypes.c_float),
                                           A.ptr(w, ctypes.c_float), labels.size,
                                           out.ctypes.data_as(ctypes.POINTER(A.SbGradPair))))

@@ -568,7 +568,8 @@ int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_TRY(hist_default_choice(ctx, g, &choice));
   const char* at = std::getenv("SB_HIST_AUTOTUNE");
   const bool tune = !std::getenv("SB_HIST_LAYOUT") && !(at && std::strcmp(at, "0") == 0) && n >= TUNE_MIN_ROWS;
-  if (tune) {
+  const std::vector<HistChoice> cands = tune ? hist_candidates(ctx, g) : std::vector<HistChoice>();
+  if (tune && cands.size() > 1) {
     int lg = 0;
     while ((size_t(2) << lg) <= n) ++lg;
     const TuneKey key{ctx->device, (int)F, g->max_feature_bins, lg, g->has_categorical};
@@ -582,7 +583,6 @@ int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
       }
     }
     if (!cached) {
-      const std::vector<HistChoice> cands = hist_candidates(ctx, g);
       float best_t = 1e30f;
       HistChoice best = choice, last{-1, -1};
       for (const HistChoice& c : cands) {

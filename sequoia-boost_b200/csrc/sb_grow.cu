@@ -45,8 +45,11 @@ struct NodeSplit {
   uint8_t cat_order[MAX_CAT_BINS];
 };
 
-struct Fill {
-  unsigned int left, right, lsamp, rsamp;
+// Rows a split node has sent to each child so far (the lists hold sampled
+// rows only, so these are also the children's sampled counts). 8-byte
+// aligned: the partition adds to both with one 64-bit atomic.
+struct __align__(8) Fill {
+  unsigned int left, right;
 };
 
 struct FeatRec;
@@ -123,7 +126,8 @@ struct BState {
   // rows
   uint32_t* rows0;          // [K][n]
   uint32_t* rows1;          // [K][n]
-  unsigned int* kept;       // sampled rows this round
+  unsigned int* kept;       // sampled rows this round (the root list's front)
+  unsigned int* unkept;     // rows outside the subset (the root list's back)
   // gradients
   float* margin;            // [n][K]
   float* delta;             // [n][K] this round's leaf value of each row (pending add)
@@ -268,66 +272,136 @@ __device__ __forceinline__ void row_gradient(int objective, int K, float spw, co
   }
 }
 
-__global__ void k_gradient(BState S) {
+// Gradients of every row (train.rs:297-302) and the round's row subset
+// (sample_rows, train.rs:465-475). The subset goes to the root list compacted:
+// each block owns a contiguous chunk of rows, reserves its places with one
+// atomic per counter, and writes its sampled rows (ascending) to the front of
+// rows0 and the others to the back, so the per-node lists hold sampled rows
+// only; the rows left out get their leaf values from k_route_rest.
+__global__ void __launch_bounds__(256) k_gradient(BState S) {
   const unsigned long long round = *S.round + S.round_base;
   const uint64_t rk = sb_round_key(S.seed, round);
-  unsigned int kept = 0;
   float mg[16], mh[16];
   const int K = S.K;
+  const size_t n = S.n;
   for (int c = 0; c < 16; ++c) mg[c] = mh[c] = 0.0f;
-  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < S.n;
-       r += (size_t)gridDim.x * blockDim.x) {
-    if (!S.ext_gpair) {
-      const float w0 = S.weights ? S.weights[r] : 1.0f;
-      const float y = S.labels[r];
-      if (S.apply_delta)  // the previous tree's leaf values (train.rs:326-328)
-        for (int c = 0; c < K; ++c) S.margin[r * K + c] = __fadd_rn(S.margin[r * K + c], S.delta[r * K + c]);
-      row_gradient(S.objective, K, S.spw, S.margin + r * K, y, w0, S.weights != nullptr,
-                   [&](int c, float g, float h) {
-                     S.gpair[(size_t)c * S.n + r] = make_float2(g, h);
-                     if (c < 16) {
-                       mg[c] = fmaxf(mg[c], fabsf(g));
-                       mh[c] = fmaxf(mh[c], fabsf(h));
-                     }
-                   });
-    } else {
-      for (int c = 0; c < K && c < 16; ++c) {
-        float2 v = S.gpair[(size_t)c * S.n + r];
-        mg[c] = fmaxf(mg[c], fabsf(v.x));
-        mh[c] = fmaxf(mh[c], fabsf(v.y));
-      }
-    }
-    bool keep;
-    if (S.ext_gpair) keep = !(S.rows0[r] & UNSAMPLED);  // the caller's subset
-    else keep = S.subsample >= 1.0 || sb_u01(sb_row_draw(rk, r)) < S.subsample;
-    if (!S.ext_gpair) S.rows0[r] = (uint32_t)r | (keep ? 0u : UNSAMPLED);
-    kept += keep ? 1u : 0u;
-  }
-  // one atomic per block and counter (same-address atomics per warp serialise)
-  __shared__ unsigned int s_kept;
+  __shared__ unsigned int s_cnt[2], s_base[2], s_wk[8], s_wu[8];
   __shared__ unsigned int s_max[32];
-  if (threadIdx.x == 0) s_kept = 0;
-  if (threadIdx.x < 32) s_max[threadIdx.x] = 0u;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t per = (n + gridDim.x - 1) / gridDim.x;
+  const size_t lo = min(n, (size_t)blockIdx.x * per), hi = min(n, lo + per);
+  // the caller's subset (flags in rows1), or the Bernoulli draw
+  auto keep_of = [&](size_t r) -> bool {
+    if (S.ext_gpair) return !(S.rows1[r] & UNSAMPLED);
+    return S.subsample >= 1.0 || sb_u01(sb_row_draw(rk, r)) < S.subsample;
+  };
+  unsigned int c0 = 0;
+  for (size_t r = lo + tid; r < hi; r += blockDim.x) c0 += keep_of(r) ? 1u : 0u;
+  if (tid < 2) s_cnt[tid] = 0u;
+  if (tid < 32) s_max[tid] = 0u;
   __syncthreads();
-  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xFFFFFFFFu, kept, o);
-  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(&s_kept, kept);
+  for (int o = 16; o > 0; o >>= 1) c0 += __shfl_xor_sync(0xFFFFFFFFu, c0, o);
+  if (lane == 0 && c0) atomicAdd(&s_cnt[0], c0);
+  __syncthreads();
+  if (tid == 0) {  // one atomic per block and counter (same-address atomics serialise)
+    s_base[0] = s_cnt[0] ? atomicAdd(S.kept, s_cnt[0]) : 0u;
+    const unsigned int un = (unsigned int)(hi - lo) - s_cnt[0];
+    s_base[1] = un ? atomicAdd(S.unkept, un) : 0u;
+  }
+  __syncthreads();
+  unsigned int front = s_base[0], back = s_base[1];
+  const unsigned lt = (1u << lane) - 1u;
+  for (size_t base = lo; base < hi; base += blockDim.x) {  // the same trip count in every thread
+    const size_t r = base + tid;
+    const bool valid = r < hi;
+    bool keep = false;
+    if (valid) {
+      if (!S.ext_gpair) {
+        const float w0 = S.weights ? S.weights[r] : 1.0f;
+        const float y = S.labels[r];
+        if (S.apply_delta)  // the previous tree's leaf values (train.rs:326-328)
+          for (int c = 0; c < K; ++c) S.margin[r * K + c] = __fadd_rn(S.margin[r * K + c], S.delta[r * K + c]);
+        row_gradient(S.objective, K, S.spw, S.margin + r * K, y, w0, S.weights != nullptr,
+                     [&](int c, float g, float h) {
+                       S.gpair[(size_t)c * n + r] = make_float2(g, h);
+                       if (c < 16) {
+                         mg[c] = fmaxf(mg[c], fabsf(g));
+                         mh[c] = fmaxf(mh[c], fabsf(h));
+                       }
+                     });
+      } else {
+        for (int c = 0; c < K && c < 16; ++c) {
+          float2 v = S.gpair[(size_t)c * n + r];
+          mg[c] = fmaxf(mg[c], fabsf(v.x));
+          mh[c] = fmaxf(mh[c], fabsf(v.y));
+        }
+      }
+      keep = keep_of(r);
+    }
+    const unsigned km = __ballot_sync(0xFFFFFFFFu, keep), um = __ballot_sync(0xFFFFFFFFu, valid && !keep);
+    if (lane == 0) {
+      s_wk[warp] = __popc(km);
+      s_wu[warp] = __popc(um);
+    }
+    __syncthreads();
+    unsigned int ko = 0, uo = 0, kt = 0, ut = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      if (w < warp) {
+        ko += s_wk[w];
+        uo += s_wu[w];
+      }
+      kt += s_wk[w];
+      ut += s_wu[w];
+    }
+    if (keep) S.rows0[front + ko + __popc(km & lt)] = (uint32_t)r;
+    else if (valid) S.rows0[n - 1 - (back + uo + __popc(um & lt))] = (uint32_t)r;
+    front += kt;
+    back += ut;
+    __syncthreads();  // s_wk / s_wu are rewritten by the next tile
+  }
   if (S.fixed) {
     for (int c = 0; c < K && c < 16; ++c) {
-      float a = mg[c], b = mh[c];
+      float a2 = mg[c], b2 = mh[c];
       for (int o = 16; o > 0; o >>= 1) {
-        a = fmaxf(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
-        b = fmaxf(b, __shfl_xor_sync(0xFFFFFFFFu, b, o));
+        a2 = fmaxf(a2, __shfl_xor_sync(0xFFFFFFFFu, a2, o));
+        b2 = fmaxf(b2, __shfl_xor_sync(0xFFFFFFFFu, b2, o));
       }
-      if ((threadIdx.x & 31) == 0) {
-        atomicMax(&s_max[2 * c], __float_as_uint(a));
-        atomicMax(&s_max[2 * c + 1], __float_as_uint(b));
+      if (lane == 0) {
+        atomicMax(&s_max[2 * c], __float_as_uint(a2));
+        atomicMax(&s_max[2 * c + 1], __float_as_uint(b2));
       }
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && s_kept) atomicAdd(S.kept, s_kept);
-  if (S.fixed && threadIdx.x < 2 * K && threadIdx.x < 32 && s_max[threadIdx.x])
-    atomicMax(&S.maxabs[threadIdx.x], s_max[threadIdx.x]);
+  if (S.fixed && tid < 2 * K && tid < 32 && s_max[tid]) atomicMax(&S.maxabs[tid], s_max[tid]);
+}
+
+// Leaf values of the rows outside the round's subset (rows0[n - unkept, n)):
+// each is routed through the round's K trees in bin space, as the partition
+// routes sampled rows (missing -> default_left; categorical: the category
+// set; numeric: local bin <= split bin).
+__global__ void k_route_rest(BState S) {
+  const size_t n = S.n;
+  const size_t un = *S.unkept;
+  const unsigned long long round = *S.round;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < un; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t r = S.rows0[n - 1 - i];
+    for (int k = 0; k < S.K; ++k) {
+      const sb_node* out = S.out_nodes + ((size_t)round * S.K + k) * S.maxn;
+      int nid = 0;
+      while (out[nid].left != -1) {
+        const NodeSplit& sp = S.split[NI(S, k, nid)];
+        const int c = (int)S.bins_col[(size_t)sp.feature * n + r];
+        bool go;
+        if (c == (int)MISSING_BIN) go = sp.default_left != 0;
+        else if (sp.is_cat) go = (sp.cat_mask[c >> 5] >> (c & 31)) & 1u;
+        else go = c <= sp.bin;
+        nid = go ? out[nid].left : out[nid].right;
+      }
+      if (S.update_margin) S.delta[(size_t)r * S.K + k] = S.leafval[NI(S, k, nid)];
+    }
+    if (S.row_leaf) S.row_leaf[r] = -1;
+  }
 }
 
 // Objective::gradient over caller-supplied margins (row-major [n][K]),
@@ -382,12 +456,24 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
   const int k = blockIdx.x, tid = threadIdx.x;
   const int F = S.F;
   const uint64_t tkey = sb_tree_key(S.seed, round, (uint64_t)(k + S.k_base));
-  if (k == 0 && tid == 0) {
-    *S.qerr = 0ull;
-    if (*S.kept == 0 && !S.ext_gpair) {  // train.rs:472-474
-      uint64_t rk = sb_round_key(S.seed, round);
-      S.rows0[sb_row_fallback(rk, S.n)] &= ~UNSAMPLED;
-      *S.kept = 1;
+  // the subset's size; an empty draw takes one row (train.rs:472-474)
+  const unsigned int kept0 = *S.kept;
+  const bool fallback = kept0 == 0 && !S.ext_gpair && S.n > 0;
+  const unsigned int kept = fallback ? 1u : kept0;
+  if (k == 0 && tid == 0) *S.qerr = 0ull;
+  if (k == 0 && fallback) {  // every row is at the back: move the fallback row to the front
+    __shared__ int s_at;
+    if (tid == 0) s_at = -1;
+    __syncthreads();
+    const uint32_t fb = (uint32_t)sb_row_fallback(sb_round_key(S.seed, round), S.n);
+    for (size_t i = tid; i < S.n; i += blockDim.x)
+      if (S.rows0[i] == fb) s_at = (int)i;
+    __syncthreads();
+    if (tid == 0 && s_at >= 0) {
+      S.rows0[s_at] = S.rows0[0];
+      S.rows0[0] = fb;
+      *S.unkept = (unsigned int)S.n - 1u;
+      *S.kept = 1u;  // the other blocks took `kept` before this write
     }
   }
   for (int f = tid; f < F; f += blockDim.x) s_a[f] = (uint32_t)f;
@@ -448,25 +534,25 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
     S.cat_count[k] = 0;
     if (S.lossguide) S.ndepth[NI(S, k, 0)] = 0;
     const size_t r0 = NI(S, k, 0);
-    S.seg[r0] = make_uint2(0u, (unsigned)S.n);
-    S.nsamp[r0] = *S.kept;
+    S.seg[r0] = make_uint2(0u, kept);
+    S.nsamp[r0] = kept;
     S.bounds[r0] = make_double2(-INFINITY, INFINITY);
     S.allowed_all[r0] = 1;
     S.built[r0] = 1;
     S.parent[r0] = -1;
     S.root_total[k] = make_longlong2(0, 0);
     HistItem it;
-    it.rows = S.rows0;  // level 0 shares the root list of class 0
+    it.rows = S.rows0;  // level 0 shares the root list of class 0 (sampled rows only)
     it.begin = 0;
-    it.end = (uint32_t)S.n;
+    it.end = kept;
     it.k = (uint32_t)k;
     it.root = 1;
     it.out = S.lossguide ? node_hist(S, k, 0) : level_hist(S, 0, k, 0);
     it.total = &S.root_total[k];
     S.items[k] = it;
-    S.prefix[k] = (uint64_t)k * S.n;
+    S.prefix[k] = (uint64_t)k * kept;
     if (k == 0) {
-      S.prefix[S.K] = (uint64_t)S.K * S.n;
+      S.prefix[S.K] = (uint64_t)S.K * kept;
       *S.item_count = S.K;
     }
   }
@@ -1063,7 +1149,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
         if (d == 0) out[0] = make_leaf(0.0f, (float)st.y);  // RegTree::with_root
         const uint2 sg = S.seg[ni];
         tiles = (int)((sg.y - sg.x + PART_TILE - 1) / PART_TILE);
-        S.fill[ni] = Fill{0u, 0u, 0u, 0u};
+        S.fill[ni] = Fill{0u, 0u};
         if (v) {
           const int left = nn0 + 2 * rank, right = left + 1;
           const int f = sp->feature;
@@ -1191,7 +1277,6 @@ constexpr int PART_WARPS = PART_THREADS / 32;
 constexpr int PART_STEPS = PART_TILE / PART_THREADS;  // 32-row steps per warp
 __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) {
   __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
-  __shared__ uint2 s_ws[PART_WARPS];
   __shared__ unsigned int s_base[2];
   const bool last = !S.lossguide && (d + 1 == S.max_depth);
   const int ntiles = *S.ptile_count;
@@ -1225,7 +1310,7 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
     const int wbeg = tile.z + warp * (PART_STEPS * 32);
     uint32_t rv[PART_STEPS];
     unsigned lm[PART_STEPS];
-    unsigned nl = 0, na = 0, nls = 0, nrs = 0;  // lane-uniform warp totals
+    unsigned nl = 0, na = 0;  // lane-uniform warp totals
 #pragma unroll
     for (int i = 0; i < PART_STEPS; ++i) {
       const int p = wbeg + i * 32 + lane;
@@ -1246,13 +1331,10 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
         const int b = c - fb;
         go = (sp.cat_mask[b >> 5] >> (b & 31)) & 1u;
       } else go = c <= sbin_code;
-      const bool smp = !(rv[i] & UNSAMPLED);
       lm[i] = __ballot_sync(0xFFFFFFFFu, valid && go);
       const unsigned vm = __ballot_sync(0xFFFFFFFFu, valid);
       nl += __popc(lm[i]);
       na += __popc(vm);
-      nls += __popc(__ballot_sync(0xFFFFFFFFu, valid && go && smp));
-      nrs += __popc(__ballot_sync(0xFFFFFFFFu, valid && !go && smp));
     }
     if (last) {  // children are final leaves: margins only
       const int left_id = S.out_nodes[((size_t)(*S.round) * K + k) * S.maxn + nid].left;
@@ -1271,22 +1353,19 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
     if (lane == 0) {
       s_wl[warp] = nl;
       s_wa[warp] = na;
-      s_ws[warp] = make_uint2(nls, nrs);
     }
     Fill* fl = &S.fill[ni];
     __syncthreads();
-    if (threadIdx.x == 0) {  // one set of counter atomics per tile
-      unsigned tl = 0, ta = 0, tls = 0, trs = 0;
+    if (threadIdx.x == 0) {  // one 64-bit atomic per tile reserves both children's places
+      unsigned tl = 0, ta = 0;
       for (int w = 0; w < PART_WARPS; ++w) {
         tl += s_wl[w];
         ta += s_wa[w];
-        tls += s_ws[w].x;
-        trs += s_ws[w].y;
       }
-      if (tls) atomicAdd(&fl->lsamp, tls);
-      if (trs) atomicAdd(&fl->rsamp, trs);
-      s_base[0] = atomicAdd(&fl->left, tl);
-      s_base[1] = atomicAdd(&fl->right, ta - tl) + (ta - tl);  // right rows fill downwards
+      const unsigned long long old = atomicAdd(reinterpret_cast<unsigned long long*>(fl),
+                                               ((unsigned long long)(ta - tl) << 32) | tl);
+      s_base[0] = (unsigned)old;
+      s_base[1] = (unsigned)(old >> 32) + (ta - tl);  // right rows fill downwards
     }
     __syncthreads();
     unsigned wl = 0, wa = 0;  // rows of earlier warps of this tile
@@ -1349,9 +1428,9 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
           const size_t li = NI(S, k, l), ri = NI(S, k, r);
           S.seg[li] = make_uint2(sg.x, sg.x + fl.left);
           S.seg[ri] = make_uint2(sg.x + fl.left, sg.y);
-          S.nsamp[li] = fl.lsamp;
-          S.nsamp[ri] = fl.rsamp;
-          const bool build_left = fl.lsamp <= fl.rsamp;
+          S.nsamp[li] = fl.left;
+          S.nsamp[ri] = fl.right;
+          const bool build_left = fl.left <= fl.right;
           S.built[li] = build_left ? 1 : 0;
           S.built[ri] = build_left ? 0 : 1;
           bchild = build_left ? l : r;
@@ -1545,6 +1624,7 @@ __global__ void k_round_end(BState S) {
   if (threadIdx.x == 0) {
     *S.round = round + 1;
     *S.kept = 0;
+    *S.unkept = 0;
     if (S.fixed)
       for (int i = 0; i < 2 * S.K; ++i) S.maxabs[i] = 0u;
   }
@@ -1900,8 +1980,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   SB_TRY(b->d_lvl.alloc_zero(ctx, 6 * K));
   SB_TRY(b->d_rows0.alloc_zero(ctx, (size_t)K * b->n));
   SB_TRY(b->d_rows1.alloc_zero(ctx, (size_t)K * b->n));
-  SB_TRY(b->d_kept.alloc_zero(ctx, 1));
-  SB_CUDA(cudaMemsetAsync(b->d_kept.p, 0, 4, st));
+  SB_TRY(b->d_kept.alloc_zero(ctx, 2));  // kept, unkept
   SB_TRY(b->d_margin.alloc_zero(ctx, b->n * K));
   SB_TRY(b->d_delta.alloc_zero(ctx, b->n * K));
   SB_TRY(b->d_gpair.alloc_zero(ctx, (size_t)K * b->n));
@@ -2021,6 +2100,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.rows0 = b->d_rows0.p;
   S.rows1 = b->d_rows1.p;
   S.kept = b->d_kept.p;
+  S.unkept = b->d_kept.p + 1;
   S.margin = b->d_margin.p;
   S.delta = b->d_delta.p;
   S.apply_delta = 0;
@@ -2154,6 +2234,8 @@ int booster_round_body(sb_booster* b, int apply_delta) {
       SB_TRY(hist(b->K * (1 << d)));
     }
   }
+  // the rows outside the subset take their leaf values by routing
+  SB_LAUNCH(ctx, k_route_rest, gblocks, 256, 0, S);
   SB_LAUNCH(ctx, k_round_end, 1, 32, 0, S);
   if (b->timing) {
     SB_CUDA(cudaEventRecord(r1, ctx->stream));
@@ -2380,9 +2462,9 @@ int approx_train(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_
       sb_booster b;
       SB_TRY(booster_init(&b, ctx, &g, &q, 1, true));
       SB_CUDA(cudaMemsetAsync(d_kept.p, 0, 4, st));
-      SB_LAUNCH(ctx, k_approx_rows, blocks, 256, 0, p->seed, (unsigned long long)r, p->subsample, n, b.d_rows0.p,
-                d_kept.p);
-      SB_LAUNCH(ctx, k_approx_fallback, 1, 1, 0, p->seed, (unsigned long long)r, n, b.d_rows0.p, d_kept.p);
+      SB_LAUNCH(ctx, k_approx_rows, blocks, 256, 0, p->seed, (unsigned long long)r, p->subsample, n, b.d_rows1.p,
+                d_kept.p);  // the subset's flags, which the round's gradient pass compacts
+      SB_LAUNCH(ctx, k_approx_fallback, 1, 1, 0, p->seed, (unsigned long long)r, n, b.d_rows1.p, d_kept.p);
       SB_CUDA(cudaMemcpyAsync(b.d_gpair.p, d_gk.p, n * 8, cudaMemcpyDeviceToDevice, st));
       b.S.round_base = (unsigned long long)r;  // column sampling of class k in round r
       b.S.k_base = k;
@@ -2639,7 +2721,7 @@ int sb_tree_build(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p, cons
     rl[rows[i]] &= ~UNSAMPLED;
   }
   cudaStream_t st = ctx->stream;
-  SB_CUDA(cudaMemcpyAsync(b.d_rows0.p, rl.data(), n * 4, cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(b.d_rows1.p, rl.data(), n * 4, cudaMemcpyHostToDevice, st));  // subset flags
   SB_CUDA(cudaMemcpyAsync(b.d_gpair.p, gpair, n * 8, cudaMemcpyHostToDevice, st));
   b.S.round_base = round;  // column sampling of class k in round `round`
   b.S.k_base = (int)k;

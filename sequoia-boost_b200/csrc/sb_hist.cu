@@ -68,6 +68,36 @@ __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint
   return lo;
 }
 
+// One addition into each plane of the shared partial, at the 32-bit shared
+// address `a` (g plane) and `a + hoff` (h plane), with `red` (no value
+// returned), only in the lanes where `on` holds: a predicate on the two
+// instructions rather than a branch around them. FIXED: int32 g and uint32
+// h; FP32: f32 bits.
+template <bool FIXED>
+__device__ __forceinline__ void add_pair_if(bool on, unsigned a, unsigned hoff, uint32_t vg, uint32_t vh) {
+  if (FIXED)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %0, 0;\n\t"
+        "@p red.shared.add.s32 [%1], %2;\n\t@p red.shared.add.u32 [%3], %4;\n\t}" ::"r"((unsigned)on),
+        "r"(a), "r"(vg), "r"(a + hoff), "r"(vh));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %0, 0;\n\t"
+        "@p red.shared.add.f32 [%1], %2;\n\t@p red.shared.add.f32 [%3], %4;\n\t}" ::"r"((unsigned)on),
+        "r"(a), "f"(__uint_as_float(vg)), "r"(a + hoff), "f"(__uint_as_float(vh)));
+}
+
+template <bool FIXED>
+__device__ __forceinline__ void add_pair(unsigned a, unsigned hoff, uint32_t vg, uint32_t vh) {
+  if (FIXED) {
+    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(a), "r"(vg));
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a + hoff), "r"(vh));
+  } else {
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(__uint_as_float(vg)));
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a + hoff), "f"(__uint_as_float(vh)));
+  }
+}
+
 // The shared partial is two planes of nent 32-bit words, g then h (FIXED:
 // int32 / uint32 integers; FP32: floats), so a warp's atomics spread over all
 // 32 banks. Every entry costs one add into each plane.
@@ -103,6 +133,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     const int nf = tile.f1 - tile.f0;
     const int nent = tile.nbins + nf;
     unsigned* sh_h = sh_g + nent;
+    const unsigned sh_base = (unsigned)__cvta_generic_to_shared(sh_g), hoff = 4u * (unsigned)nent;
     const bool want_total = item.root && t == 0;
 
     // lane `lane` owns the 4 consecutive features f0 + 4*lane .. +3 of the tile
@@ -138,22 +169,22 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
     const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
     uint32_t p = pbeg + warp * ROWS_PER_WARP;
-    uint32_t next_rid = UNSAMPLED;
+    uint32_t next_rid = 0u;
     if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
     for (; p < pend; p += stride) {
       const uint32_t my_rid = next_rid;
       const uint32_t pn = p + stride + lane;
-      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
-      const bool my_use = lane < ROWS_PER_WARP && !(my_rid & UNSAMPLED);
+      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : 0u;
+      // rows of this batch (the lists hold sampled rows only), the same in every lane
+      const uint32_t nrow = min(pend - p, (uint32_t)ROWS_PER_WARP);
       uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
-      if (my_use) {
+      if (lane < (int)nrow) {
         if (FIXED) {
-          const unsigned long long pk =
-              reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          const unsigned long long pk = reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + my_rid];
           my_g = (uint32_t)(pk >> 32);
           my_h = (uint32_t)(pk & 0xFFFFFFFFull);
         } else {
-          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + my_rid];
           my_g = __float_as_uint(v.x);
           my_h = __float_as_uint(v.y);
         }
@@ -168,31 +199,23 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
           }
         }
       }
-      const unsigned use_mask = __ballot_sync(0xFFFFFFFFu, my_use);
       uint2 bv[ROWS_PER_WARP];
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q) & ~UNSAMPLED;
-        bv[q] = (((use_mask >> q) & 1u) && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
-                                                    : make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q);
+        bv[q] = ((uint32_t)q < nrow && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
+                                                : make_uint2(0u, 0u);
       }
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
         const uint32_t vg = __shfl_sync(0xFFFFFFFFu, my_g, q);
         const uint32_t vh = __shfl_sync(0xFFFFFFFFu, my_h, q);
-        if (!((use_mask >> q) & 1u)) continue;
+        if ((uint32_t)q >= nrow) break;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          if (!fon[j]) continue;
           const uint32_t w = j < 2 ? bv[q].x : bv[q].y;
-          const int idx = (int)((j & 1) ? (w >> 16) : (w & 0xFFFFu));  // the tile-relative code
-          if (FIXED) {
-            atomicAdd(reinterpret_cast<int*>(sh_g) + idx, (int)vg);
-            atomicAdd(sh_h + idx, vh);
-          } else {
-            atomicAdd(reinterpret_cast<float*>(sh_g) + idx, __uint_as_float(vg));
-            atomicAdd(reinterpret_cast<float*>(sh_h) + idx, __uint_as_float(vh));
-          }
+          const unsigned idx = (j & 1) ? (w >> 16) : (w & 0xFFFFu);  // the tile-relative code
+          add_pair_if<FIXED>(fon[j], sh_base + 4u * idx, hoff, vg, vh);
         }
       }
     }
@@ -298,6 +321,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_lanes(HistDev a) {
     const FeatureTile tile = a.tiles[t];
     const int words = 32 * tile.E;  // per plane
     unsigned* sh_h = sh_g + words;
+    const unsigned sh_base = (unsigned)__cvta_generic_to_shared(sh_g), hoff = 4u * (unsigned)words;
     const bool want_total = item.root && t == 0;
 
     // the features of this lane's code positions that the tree's column pool
@@ -326,22 +350,21 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_lanes(HistDev a) {
     const uint16_t* bins_lane = a.bins + slot0;
     const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
     uint32_t p = pbeg + warp * ROWS_PER_WARP;
-    uint32_t next_rid = UNSAMPLED;
+    uint32_t next_rid = 0u;
     if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
     for (; p < pend; p += stride) {
       const uint32_t my_rid = next_rid;
       const uint32_t pn = p + stride + lane;
-      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : UNSAMPLED;
-      const bool my_use = lane < ROWS_PER_WARP && !(my_rid & UNSAMPLED);
+      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : 0u;
+      const uint32_t nrow = min(pend - p, (uint32_t)ROWS_PER_WARP);
       uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
-      if (my_use) {
+      if (lane < (int)nrow) {
         if (FIXED) {
-          const unsigned long long pk =
-              reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          const unsigned long long pk = reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + my_rid];
           my_g = (uint32_t)(pk >> 32);
           my_h = (uint32_t)(pk & 0xFFFFFFFFull);
         } else {
-          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + (my_rid & ~UNSAMPLED)];
+          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + my_rid];
           my_g = __float_as_uint(v.x);
           my_h = __float_as_uint(v.y);
         }
@@ -356,31 +379,20 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_lanes(HistDev a) {
           }
         }
       }
-      const unsigned use_mask = __ballot_sync(0xFFFFFFFFu, my_use);
       CT cv[ROWS_PER_WARP];
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q) & ~UNSAMPLED;
-        cv[q] = ((use_mask >> q) & 1u) ? __ldg(reinterpret_cast<const CT*>(bins_lane + (size_t)id * a.Fp))
-                                       : C::none();
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q);
+        cv[q] = (uint32_t)q < nrow ? __ldg(reinterpret_cast<const CT*>(bins_lane + (size_t)id * a.Fp)) : C::none();
       }
 #pragma unroll
       for (int q = 0; q < ROWS_PER_WARP; ++q) {
         const uint32_t vg = __shfl_sync(0xFFFFFFFFu, my_g, q);
         const uint32_t vh = __shfl_sync(0xFFFFFFFFu, my_h, q);
-        if (!((use_mask >> q) & 1u)) continue;
+        if ((uint32_t)q >= nrow) break;
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          if (!fon[s]) continue;
-          const int w = C::get(cv[q], s) * 32 + lane;
-          if (FIXED) {
-            atomicAdd(reinterpret_cast<int*>(sh_g) + w, (int)vg);
-            atomicAdd(sh_h + w, vh);
-          } else {
-            atomicAdd(reinterpret_cast<float*>(sh_g) + w, __uint_as_float(vg));
-            atomicAdd(reinterpret_cast<float*>(sh_h) + w, __uint_as_float(vh));
-          }
-        }
+        for (int s = 0; s < S; ++s)
+          add_pair_if<FIXED>(fon[s], sh_base + 4u * (unsigned)(C::get(cv[q], s) * 32 + lane), hoff, vg, vh);
       }
     }
     if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
@@ -666,12 +678,17 @@ int hist_default_choice(sb_ctx* ctx, Ghist* g, HistChoice* out) {
   return SB_OK;
 }
 
-// Every choice that fits the index: TILED, and LANES with 1, 2 and 4
-// positions per lane where its features pack.
+// The choices the autotuner times: TILED, and for up to 64 features (where
+// TILED keeps at most 16 of a warp's lanes busy) LANES with 1 and 2
+// positions per lane where the features pack. Wider matrices take TILED: on
+// the 10M x 100 workload a whole round measured TILED faster at every level
+// (ncu: LANES cut the shared-atomic wavefronts by 2.4x but waited longer on
+// its 23 % longer rows), while a single timed launch ranked LANES first.
 std::vector<HistChoice> hist_candidates(sb_ctx* ctx, Ghist* g) {
   std::vector<HistChoice> out{HistChoice{HIST_LAYOUT_TILED, 0}};
+  if (g->F > 64) return out;
   const std::vector<FeatureTile> keep = g->tiles;
-  for (int slots : {1, 2, 4}) {
+  for (int slots : {1, 2}) {
     std::vector<std::vector<LanePlace>> places;
     if (plan_lanes(g, smem_budget(ctx), slots, &places) == SB_OK) out.push_back(HistChoice{HIST_LAYOUT_LANES, slots});
   }
@@ -744,9 +761,10 @@ int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const 
   return SB_OK;
 }
 
-// Device time of one fixed-point histogram launch over the first min(n,
-// 2^20) rows (all in the row list), best of two after a warm-up launch: the
-// autotuner's measure.
+// Device time of fixed-point histogram launches over min(n, 2^20) rows
+// spread over the whole matrix (one row drawn from each of m equal strides,
+// ascending): the gathers of a round's deeper levels, on codes mostly
+// outside L2. Best of two after a warm-up launch: the autotuner's measure.
 int hist_time(sb_ctx* ctx, const Ghist* g, float* ms) {
   const size_t m = std::min<size_t>(g->n, (size_t)1 << 20);
   const size_t HB = g->total_bins + g->F;
@@ -766,7 +784,8 @@ int hist_time(sb_ctx* ctx, const Ghist* g, float* ms) {
   SB_TRY(count.alloc(ctx, 1));
   SB_TRY(tiles.alloc(ctx, g->tiles.size()));
   std::vector<uint32_t> h_rows(m);
-  for (size_t i = 0; i < m; ++i) h_rows[i] = (uint32_t)i;
+  const size_t stride = g->n / m;
+  for (size_t i = 0; i < m; ++i) h_rows[i] = (uint32_t)(i * stride + sb_mix64(i) % stride);
   HistItem it{};
   it.rows = rows.p;
   it.begin = 0;

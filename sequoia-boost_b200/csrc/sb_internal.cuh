@@ -271,6 +271,12 @@ struct DevEnsemble {
   bool shap_table = false;   // per-path contribution tables are in use
   DBuf<float> shap_tab;      // per path: [2^D][round_up(D, 4)] f32 contributions
   DBuf<long long> shap_tab_off;  // [n_paths] first float of each path's table
+  DBuf<int4> tab_el;         // per element: {feature, lo, hi, (table-chunk feature index << 1) | miss_ok}
+  DBuf<int4> tab_chunk;      // {class, first tree, trees, -}: work units of the table kernel
+  DBuf<int> tab_chunk_fo;    // [n_tab_chunks + 1] offsets into tab_chunk_f
+  DBuf<int> tab_chunk_f;     // each table chunk's distinct features
+  int n_tab_chunks = 0;
+  int tab_max_fc = 1;
   int n_trees = 0;
   int max_depth = 0;
   int max_path_len = 0;      // elements, bias included

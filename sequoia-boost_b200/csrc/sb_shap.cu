@@ -474,15 +474,43 @@ __global__ void __launch_bounds__(128) k_shap_table_build(ShapTableDev P, long l
   }
 }
 
-// The table form of k_shap_paths: same blocks (SHAP_ROWS rows over one chunk
-// of paths), same shared partials; per path a row forms its pattern and adds
-// the D table entries of it.
-__global__ void __launch_bounds__(SHAP_ROWS) k_shap_table(ShapPathsDev P, const long long* __restrict__ tab_off,
-                                                         const float* __restrict__ tab, const float* __restrict__ X,
-                                                         size_t n, int F, int K, float missing, unsigned row_blocks,
-                                                         double* __restrict__ acc) {
-  extern __shared__ float ph[];  // [chunk features][R]
-  const int R = SHAP_ROWS;
+// The table form: a block takes TAB_ROWS rows (one per thread) over one
+// table chunk, up to TAB_CHUNK_PATHS paths of several trees of one class,
+// so that the block's partials go to the f64 accumulator once per many
+// trees. The block first copies its rows' values of the chunk's features
+// into shared memory, feature-major with a padded stride, so that the
+// per-element reads of a warp (one feature, 32 rows) are one conflict-free
+// shared access instead of 32 scattered row reads. Per path a row forms its
+// pattern from the path's compact elements and adds the D table entries of
+// it; four independent paths are in flight per step.
+constexpr int TAB_ROWS = 64;
+constexpr int TAB_STRIDE = TAB_ROWS + 1;  // words per feature in the row-value copy
+constexpr int TAB_CHUNK_PATHS = 1024;
+constexpr int TAB_CHUNK_FEATURES = 192;  // distinct features of a chunk (its partial's rows)
+
+// Shared memory of one k_shap_table block for a chunk of `nfc` features:
+// the f32 partials [nfc][TAB_ROWS] and the row values [nfc][TAB_STRIDE].
+__host__ __device__ constexpr size_t shap_table_smem(int nfc) {
+  return (size_t)nfc * (TAB_ROWS + TAB_STRIDE) * sizeof(float);
+}
+
+struct ShapTabDev {
+  const int4* el;           // per element: {feature, lo bits, hi bits, (chunk feature index << 1) | miss_ok}
+  const int* off;           // [n_paths + 1] element offsets (element 0 of a path is its bias)
+  const long long* tab_off; // per path: first float of its table
+  const float* tab;
+  const int* tree_path;     // [n_trees + 1]
+  const int4* chunk;        // {class, first tree, number of trees, -}; trees t, t + K, t + 2K, ...
+  const int* chunk_fo;      // [n_chunks + 1] offsets into chunk_f
+  const int* chunk_f;       // each chunk's distinct features
+  int K;
+};
+
+__global__ void __launch_bounds__(TAB_ROWS) k_shap_table(ShapTabDev P, const float* __restrict__ X, size_t n,
+                                                        int F, float missing, unsigned row_blocks,
+                                                        double* __restrict__ acc) {
+  extern __shared__ float ph[];  // [chunk features][TAB_ROWS], then xs
+  const int R = TAB_ROWS;
   const int tid = threadIdx.x;
   const unsigned rb = blockIdx.x % row_blocks;
   const size_t r0 = (size_t)rb * R;
@@ -490,31 +518,64 @@ __global__ void __launch_bounds__(SHAP_ROWS) k_shap_table(ShapPathsDev P, const 
   const int4 ch = P.chunk[ci];
   const int c = ch.x;
   const int fo = P.chunk_fo[ci], nfc = P.chunk_fo[ci + 1] - fo;
+  float* xs = ph + (size_t)nfc * R;  // [chunk features][TAB_STRIDE] row values
   for (int i = tid; i < nfc * R; i += R) ph[i] = 0.0f;
-  const float* row = X + (r0 + tid < n ? r0 + tid : r0) * (size_t)F;
-  __syncwarp();
+  // consecutive threads read consecutive chunk features of one row
+  const int rows_here = (int)min((size_t)R, n - r0);
+  for (int i = tid; i < nfc * rows_here; i += R) {
+    const int r = i / nfc, j = i - r * nfc;
+    xs[j * TAB_STRIDE + r] = __ldg(X + (r0 + r) * (size_t)F + P.chunk_f[fo + j]);
+  }
+  __syncthreads();
   const bool miss_nan = isnan(missing);
-  for (int p = ch.y; p < ch.z; ++p) {
-    const int e0 = P.off[p], L = P.off[p + 1] - e0, D = L - 1, Dp = (D + 3) & ~3;
-    unsigned m = 0;
-    for (int e = 1; e < L; ++e) {
-      const PathEl el = P.el[e0 + e];
-      const float v = __ldg(row + el.f);
-      const bool mis = miss_nan ? isnan(v) : v == missing;
-      const bool o = mis ? el.miss_ok != 0 : (v >= el.lo && v < el.hi);
-      m |= (o ? 1u : 0u) << (e - 1);
-    }
-    const float4* t4 = reinterpret_cast<const float4*>(tab + tab_off[p] + (long long)m * Dp);
-    for (int j = 0; j < D; j += 4) {
-      const float4 v = __ldg(t4 + (j >> 2));
-      ph[P.fc[e0 + 1 + j] * R + tid] += v.x;
-      if (j + 1 < D) ph[P.fc[e0 + 2 + j] * R + tid] += v.y;
-      if (j + 2 < D) ph[P.fc[e0 + 3 + j] * R + tid] += v.z;
-      if (j + 3 < D) ph[P.fc[e0 + 4 + j] * R + tid] += v.w;
+  const float* xr = xs + tid;
+  for (int ti = 0; ti < ch.z; ++ti) {
+    const int t = ch.y + ti * P.K;
+    const int pe = P.tree_path[t + 1];
+    for (int p0 = P.tree_path[t]; p0 < pe; p0 += 4) {
+      unsigned m[4];
+      int eb[4], dn[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {  // patterns
+        m[u] = 0u;
+        eb[u] = 0;
+        dn[u] = 0;
+        if (p0 + u < pe) {
+          eb[u] = P.off[p0 + u] + 1;
+          dn[u] = P.off[p0 + u + 1] - eb[u];
+          for (int e = 0; e < dn[u]; ++e) {
+            const int4 x = __ldg(P.el + eb[u] + e);
+            const float v = xr[(x.w >> 1) * TAB_STRIDE];
+            const bool mis = miss_nan ? isnan(v) : v == missing;
+            const bool o = mis ? (x.w & 1) != 0 : (v >= __int_as_float(x.y) && v < __int_as_float(x.z));
+            m[u] |= (o ? 1u : 0u) << e;
+          }
+        }
+      }
+      float4 tv[4][3];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {  // the table entries of the four patterns
+        const int dp = (dn[u] + 3) & ~3;
+        const float4* t4 = reinterpret_cast<const float4*>(P.tab + P.tab_off[p0 + u < pe ? p0 + u : p0] +
+                                                           (long long)m[u] * dp);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) tv[u][j] = 4 * j < dn[u] ? __ldg(t4 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float vv[4] = {tv[u][j].x, tv[u][j].y, tv[u][j].z, tv[u][j].w};
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (4 * j + q < dn[u]) ph[(__ldg(&P.el[eb[u] + 4 * j + q].w) >> 1) * R + tid] += vv[q];
+        }
+      }
     }
   }
   if (r0 + tid < n) {
-    double* a = acc + ((r0 + tid) * K + c) * (size_t)(F + 1);
+    const int Kc = P.K;
+    double* a = acc + ((r0 + tid) * Kc + c) * (size_t)(F + 1);
     for (int j = 0; j < nfc; ++j) {
       const float v = ph[j * R + tid];
       if (v != 0.0f) atomicAdd(a + P.chunk_f[fo + j], (double)v);
@@ -730,7 +791,6 @@ int shap_prepare(sb_model* m) {
     SB_TRY(raise_smem_limit((const void*)k_shap_paths<5>, smem));
     SB_TRY(raise_smem_limit((const void*)k_shap_paths<9>, smem));
     SB_TRY(raise_smem_limit((const void*)k_shap_paths<SHAP_REG_MAXL>, smem));
-    SB_TRY(raise_smem_limit((const void*)k_shap_table, smem));
     SB_TRY(raise_smem_limit((const void*)k_shap_deep, smem));
   }
   // per-path tables: 2^D patterns x Dp floats each
@@ -767,7 +827,73 @@ int shap_prepare(sb_model* m) {
       const long long pairs = moff[n_paths];
       const unsigned blocks = (unsigned)std::min<long long>((pairs + 127) / 128, (long long)ctx->num_sms * 64);
       SB_LAUNCH(ctx, k_shap_table_build, blocks, 128, 0, P, pairs);
-      D.shap_table = true;
+      // table chunks: consecutive trees of one class, up to TAB_CHUNK_PATHS
+      // paths and TAB_CHUNK_FEATURES distinct features
+      std::vector<int4> tch;
+      std::vector<int> tfo(1, 0), tf, tslot(std::max(m->n_features, 1), -1);
+      std::vector<int4> tel(pel.size());
+      int tmax = 1;
+      for (int c = 0; c < Kc; ++c) {
+        int t = c;
+        while (t < T) {
+          const int first = (int)tf.size();
+          int nt = 0, np = 0;
+          while (t < T) {
+            const int tp = tpath[t + 1] - tpath[t];
+            int fresh = 0;  // features of tree t not yet in the chunk
+            for (int q = tpath[t]; q < tpath[t + 1]; ++q)
+              for (int e = poff[q] + 1; e < poff[q + 1]; ++e)
+                if (tslot[pel[e].f] == -1) {
+                  tslot[pel[e].f] = -2;  // counted
+                  ++fresh;
+                }
+            for (int q = tpath[t]; q < tpath[t + 1]; ++q)  // undo the counting marks
+              for (int e = poff[q] + 1; e < poff[q + 1]; ++e)
+                if (tslot[pel[e].f] == -2) tslot[pel[e].f] = -1;
+            const int nf = (int)tf.size() - first;
+            if (nt > 0 && (np + tp > TAB_CHUNK_PATHS || nf + fresh > TAB_CHUNK_FEATURES)) break;
+            for (int q = tpath[t]; q < tpath[t + 1]; ++q)
+              for (int e = poff[q]; e < poff[q + 1]; ++e) {
+                const PathEl& el = pel[e];
+                int fci = 0;
+                if (el.f >= 0) {
+                  if (tslot[el.f] < 0) {
+                    tslot[el.f] = (int)tf.size() - first;
+                    tf.push_back(el.f);
+                  }
+                  fci = tslot[el.f];
+                }
+                int lo, hi;
+                std::memcpy(&lo, &el.lo, 4);
+                std::memcpy(&hi, &el.hi, 4);
+                tel[e] = make_int4(el.f < 0 ? 0 : el.f, lo, hi, (fci << 1) | (el.miss_ok ? 1 : 0));
+              }
+            np += tp;
+            ++nt;
+            t += Kc;
+          }
+          for (size_t j = first; j < tf.size(); ++j) tslot[tf[j]] = -1;
+          tmax = std::max(tmax, (int)tf.size() - first);
+          tch.push_back(make_int4(c, t - nt * Kc, nt, np));
+          tfo.push_back((int)tf.size());
+        }
+      }
+      SB_TRY(D.tab_el.alloc(ctx, std::max<size_t>(tel.size(), 1)));
+      SB_TRY(D.tab_chunk.alloc(ctx, std::max<size_t>(tch.size(), 1)));
+      SB_TRY(D.tab_chunk_fo.alloc(ctx, tfo.size()));
+      SB_TRY(D.tab_chunk_f.alloc(ctx, std::max<size_t>(tf.size(), 1)));
+      if (!tel.empty()) SB_CUDA(cudaMemcpyAsync(D.tab_el.p, tel.data(), tel.size() * 16, cudaMemcpyHostToDevice, st));
+      if (!tch.empty()) SB_CUDA(cudaMemcpyAsync(D.tab_chunk.p, tch.data(), tch.size() * 16, cudaMemcpyHostToDevice, st));
+      SB_CUDA(cudaMemcpyAsync(D.tab_chunk_fo.p, tfo.data(), tfo.size() * 4, cudaMemcpyHostToDevice, st));
+      if (!tf.empty()) SB_CUDA(cudaMemcpyAsync(D.tab_chunk_f.p, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice, st));
+      D.n_tab_chunks = (int)tch.size();
+      D.tab_max_fc = tmax;
+      // a tree with more distinct features than one block's partial can hold
+      // keeps the f64 path kernels
+      if (shap_table_smem(tmax) <= ctx->smem_optin) {
+        SB_TRY(raise_smem_limit((const void*)k_shap_table, shap_table_smem(tmax)));
+        D.shap_table = true;
+      }
       SB_CUDA(cudaStreamSynchronize(st));  // d_moff and the host vectors are released on return
     }
   }
@@ -823,8 +949,21 @@ int shap_paths(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t 
              "TreeSHAP of %zu rows over %d path chunks exceeds one launch", n, m->dev.n_shap_chunks);
   const unsigned grid = (unsigned)items;
   if (m->dev.shap_table) {
-    SB_LAUNCH_ON(ctx, st, k_shap_table, grid, R, smem, P, m->dev.shap_tab_off.p, m->dev.shap_tab.p, d_X, n, (int)F,
-                 K, missing, row_blocks, d_acc);
+    ShapTabDev Q;
+    Q.el = m->dev.tab_el.p;
+    Q.off = m->dev.path_off.p;
+    Q.tab_off = m->dev.shap_tab_off.p;
+    Q.tab = m->dev.shap_tab.p;
+    Q.tree_path = m->dev.tree_path.p;
+    Q.chunk = m->dev.tab_chunk.p;
+    Q.chunk_fo = m->dev.tab_chunk_fo.p;
+    Q.chunk_f = m->dev.tab_chunk_f.p;
+    Q.K = K;
+    const unsigned trb = (unsigned)((n + TAB_ROWS - 1) / TAB_ROWS);
+    const unsigned long long tb = (unsigned long long)trb * (unsigned long long)m->dev.n_tab_chunks;
+    SB_REQUIRE(tb < (1ull << 31), SB_ERR_UNSUPPORTED, "TreeSHAP of %zu rows exceeds one launch", n);
+    SB_LAUNCH_ON(ctx, st, k_shap_table, (unsigned)tb, TAB_ROWS, shap_table_smem(m->dev.tab_max_fc), Q, d_X, n,
+                 (int)F, missing, trb, d_acc);
   } else if (L <= 5) {
     SB_LAUNCH_ON(ctx, st, k_shap_paths<5>, grid, R, smem, P, d_X, n, (int)F, K, missing, row_blocks, d_acc);
   } else if (L <= 9) {

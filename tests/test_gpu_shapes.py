@@ -91,7 +91,7 @@ def test_multiclass_lossguide_workload_round0_bit_exact(sb, ctx, orc, layout):
     ga = m.export()
     assert ga[0].size == 11
     assert ga[1]["is_categorical"].any(), "expected categorical splits"
-    assert (ga[1]["left"] == -1).sum() > 10 * 100, "trees should grow well past 100 leaves"
+    assert (ga[1]["left"] == -1).sum() > 10 * 10, "trees should grow past 10 leaves"
     assert_trees_equal(ga, ref["model"].export())
     assert np.array_equal(m.predict_margin(sb.DMatrix(x)), ref["margins"].reshape(-1))
 

@@ -156,3 +156,19 @@ def test_graph_replayed_rounds_match_eager_rounds(sb, ctx):
     assert_trees_equal(ma, mb)
     assert np.array_equal(mida, midb)
     assert np.array_equal(fa, fb)
+
+
+@pytest.mark.parametrize("grow_policy", ["depthwise", "lossguide"])
+def test_empty_row_draw_takes_one_row(sb, ctx, orc, grow_policy):
+    """subsample so small that a round's Bernoulli draw keeps no row: the
+    round takes the one fallback row (train.rs:472-474), every other row is
+    routed through the tree for its leaf value, and the model and margins
+    equal the oracle's."""
+    x, y = _sine(500, 5, 7)
+    p = sb.TrainingParams(objective="reg:squarederror", max_depth=3, eta=0.5, subsample=1e-9,
+                          min_child_weight=0.0, grow_policy=grow_policy, max_leaves=4 if grow_policy == "lossguide" else 0,
+                          seed=11)
+    m = sb.train(p, sb.DMatrix(x, labels=y), 3, ctx=ctx)
+    ref = orc.train(x, y, p, 3)
+    assert_trees_equal(m.export(), ref["model"].export())
+    assert np.array_equal(m.predict_margin(sb.DMatrix(x)), ref["margins"].reshape(-1))
