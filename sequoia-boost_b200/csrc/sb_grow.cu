@@ -159,7 +159,7 @@ struct BState {
   int* upool_len;           // [K]
   uint32_t* pool_mask;      // [K][FW] bitmask of upool
   const uint32_t* usable;   // [FW] features with >= 2 bins
-  uint32_t* samp_scratch;   // [1024][F] when per-node sampling is on
+  uint32_t* samp_scratch;   // [max(1024, K)][F] when per-node sampling is on
   double* mbuf;             // [K][maxw][F] phase-1 best gain per (node, feature)
   // outputs
   sb_node* out_nodes;       // [tree_cap][maxn]
@@ -460,7 +460,10 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
   const unsigned int kept0 = *S.kept;
   const bool fallback = kept0 == 0 && !S.ext_gpair && S.n > 0;
   const unsigned int kept = fallback ? 1u : kept0;
-  if (k == 0 && tid == 0) *S.qerr = 0ull;
+  if (k == 0 && tid == 0) {
+    *S.qerr = 0ull;
+    *S.ptile_count = 0;  // k_assign's blocks reserve the round's first tiles from 0
+  }
   if (k == 0 && fallback) {  // every row is at the back: move the fallback row to the front
     __shared__ int s_at;
     if (tid == 0) s_at = -1;
@@ -1121,11 +1124,20 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
   __shared__ uint2 s_seg[1024];
   const unsigned long long round = *S.round;
   const int tid = threadIdx.x;
-  if (tid == 0) s_tile_carry = 0;
-  __syncthreads();
   const bool last = !S.lossguide && (d + 1 == S.max_depth);
-  for (int k = 0; k < S.K; ++k) {
+  for (int k = blockIdx.x; k < S.K; k += gridDim.x) {  // one class tree per block
     const int begin = S.lvl_begin[k], cnt = S.lvl_count[k], nn0 = S.num_nodes[k];
+    if (write_tiles) {  // reserve the tree's partition tiles (their order in the list is free)
+      int mine = 0;
+      for (int q = tid; q < cnt; q += blockDim.x) {
+        const uint2 sg = S.seg[NI(S, k, begin + q)];
+        mine += (int)((sg.y - sg.x + PART_TILE - 1) / PART_TILE);
+      }
+      int all;
+      block_scan_excl<int>(mine, &all, sm_i);
+      if (tid == 0) s_tile_carry = all ? atomicAdd(S.ptile_count, all) : 0;
+      __syncthreads();
+    }
     const size_t t = (size_t)round * S.K + k;
     sb_node* out = S.out_nodes + t * S.maxn;
     uint32_t* ocats = S.out_cats ? S.out_cats + t * S.cat_cap : nullptr;
@@ -1202,7 +1214,9 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
           S.built[ri] = 0;
           S.split[li].valid = 0;
           S.split[ri].valid = 0;
-          uint32_t* scratch = S.samp_scratch ? S.samp_scratch + (size_t)tid * S.F : nullptr;
+          // the launch has at most 1024 threads in all when per-node sampling is on
+          uint32_t* scratch =
+              S.samp_scratch ? S.samp_scratch + ((size_t)blockIdx.x * blockDim.x + tid) * S.F : nullptr;
           if (!last) {
             node_feature_mask(S, k, left, tkey, S.fmask + li * S.FW, S.allowed + li * S.FW, call, scratch);
             node_feature_mask(S, k, right, tkey, S.fmask + ri * S.FW, S.allowed + ri * S.FW, call, scratch);
@@ -1262,7 +1276,6 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
     }
     __syncthreads();
   }
-  if (tid == 0) *S.ptile_count = min(s_tile_carry, S.ptile_cap);
 }
 
 // K7 + K8: partition every split node's rows into its two children (left rows
@@ -1279,7 +1292,7 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
   __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
   __shared__ unsigned int s_base[2];
   const bool last = !S.lossguide && (d + 1 == S.max_depth);
-  const int ntiles = *S.ptile_count;
+  const int ntiles = min(*S.ptile_count, S.ptile_cap);
   // lossguide: from the tree's list into the scratch list (k_lg_copy moves it back)
   const uint32_t* rows_cur_all = (!S.lossguide && (d & 1)) ? S.rows1 : S.rows0;
   uint32_t* rows_nxt_all = (!S.lossguide && (d & 1)) ? S.rows0 : S.rows1;
@@ -1394,10 +1407,12 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
 // child to build (hist.rs:352-362: left when left_rows <= right_rows), and
 // the histogram work list of level d + 1.
 __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
+  constexpr int GROUP = 1024;  // class trees per pass over the (tree, node) pairs
   __shared__ int sm_i[33];
   __shared__ unsigned long long sm_u[33];
   __shared__ int s_items;
   __shared__ unsigned long long s_pos;
+  __shared__ int s_off[GROUP + 1];
   const int tid = threadIdx.x;
   if (tid == 0) {
     s_items = 0;
@@ -1406,22 +1421,36 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
   __syncthreads();
   const unsigned long long round = *S.round;
   const int dn = d + 1;
-  for (int k = 0; k < S.K; ++k) {
-    const int pbegin = S.prev_begin[k];
-    const int pcount = S.prev_count[k];  // frontier of level d
-    const int cbegin = S.lvl_begin[k];
-    uint32_t* rows_nxt = ((!S.lossguide && (dn & 1)) ? S.rows1 : S.rows0) + (size_t)k * S.n;
-    const sb_node* out = S.out_nodes + ((size_t)round * S.K + k) * S.maxn;
-    for (int c0 = 0; c0 < pcount; c0 += blockDim.x) {
-      const int slot = c0 + tid;
-      int v = 0;
+  for (int k0 = 0; k0 < S.K; k0 += GROUP) {
+    const int nk = min(GROUP, S.K - k0);
+    // offsets of the group's frontiers in its list of (tree, node) pairs
+    int base = 0;  // the same in every thread
+    for (int j0 = 0; j0 < nk; j0 += blockDim.x) {
+      const int j = j0 + tid;
+      int tot;
+      const int o = block_scan_excl<int>(j < nk ? S.prev_count[k0 + j] : 0, &tot, sm_i);
+      if (j < nk) s_off[j] = base + o;
+      base += tot;
+    }
+    if (tid == 0) s_off[nk] = base;
+    __syncthreads();
+    const int pairs = s_off[nk];
+    for (int c0 = 0; c0 < pairs; c0 += blockDim.x) {
+      const int q = c0 + tid;
+      int v = 0, k = k0, bchild = -1;
       unsigned long long len = 0;
-      int bchild = -1;
       uint2 bseg = make_uint2(0, 0);
-      if (slot < pcount) {
-        const int nid = pbegin + slot;
+      if (q < pairs) {
+        int lo = 0, hi = nk;  // the last tree whose offset is <= q
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_off[mid] <= q) lo = mid; else hi = mid;
+        }
+        k = k0 + lo;
+        const int nid = S.prev_begin[k] + (q - s_off[lo]);
         const size_t ni = NI(S, k, nid);
         if (S.split[ni].valid) {
+          const sb_node* out = S.out_nodes + ((size_t)round * S.K + k) * S.maxn;
           const Fill fl = S.fill[ni];
           const uint2 sg = S.seg[ni];
           const int l = out[nid].left, r = l + 1;
@@ -1445,12 +1474,12 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
       const unsigned long long pos = s_pos + block_scan_excl<unsigned long long>(len, &tot_len, sm_u);
       if (v) {
         HistItem it;
-        it.rows = rows_nxt;
+        it.rows = ((!S.lossguide && (dn & 1)) ? S.rows1 : S.rows0) + (size_t)k * S.n;
         it.begin = bseg.x;
         it.end = bseg.y;
         it.k = (uint32_t)k;
         it.root = 0;
-        it.out = S.lossguide ? node_hist(S, k, bchild) : level_hist(S, dn, k, bchild - cbegin);
+        it.out = S.lossguide ? node_hist(S, k, bchild) : level_hist(S, dn, k, bchild - S.lvl_begin[k]);
         it.total = nullptr;
         S.items[idx] = it;
         S.prefix[idx] = pos;
@@ -1466,6 +1495,7 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
   if (tid == 0) {
     *S.item_count = s_items;
     S.prefix[s_items] = s_pos;
+    *S.ptile_count = 0;  // the partition has consumed this level's tiles
   }
 }
 
@@ -1575,7 +1605,7 @@ __global__ void __launch_bounds__(256) k_lg_heap(BState S, int init) {
 
 // The expanded node's partitioned rows back into the tree's row list.
 __global__ void k_lg_copy(BState S) {
-  const int ntiles = *S.ptile_count;
+  const int ntiles = min(*S.ptile_count, S.ptile_cap);
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tile = S.ptiles[t];
     const size_t base = (size_t)tile.x * S.n;
@@ -2024,7 +2054,9 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
     SB_TRY(b->d_usable.alloc_zero(ctx, FW));
     SB_CUDA(cudaMemcpyAsync(b->d_usable.p, usable.data(), FW * 4, cudaMemcpyHostToDevice, st));
   }
-  if (p->colsample_bylevel < 1.0 || p->colsample_bynode < 1.0) SB_TRY(b->d_samp.alloc_zero(ctx, (size_t)1024 * F));
+  // per-node sampling scratch: one row per k_assign thread (1024 in all) and per class tree (k_round_prep)
+  if (p->colsample_bylevel < 1.0 || p->colsample_bynode < 1.0)
+    SB_TRY(b->d_samp.alloc_zero(ctx, (size_t)std::max(1024, K) * F));
   SB_TRY(b->d_tiles.alloc_zero(ctx, g->tiles.size()));
   SB_CUDA(cudaMemcpyAsync(b->d_tiles.p, g->tiles.data(), g->tiles.size() * sizeof(FeatureTile),
                           cudaMemcpyHostToDevice, st));
@@ -2142,6 +2174,20 @@ size_t eval_smem(const sb_booster* b) {
 // The launches of one boosting round on the context stream (also recorded into
 // a CUDA graph by booster_round). Work sizes live in device memory, so the
 // sequence depends only on the booster's shape.
+// Blocks of a partition launch: its tiles (PART_TILE rows of one node; the
+// nodes' rows are at most n per class tree) up to eight per SM.
+static unsigned part_blocks(sb_ctx* ctx, size_t n, int K, size_t nodes) {
+  const size_t tiles = (n * (size_t)K + PART_TILE - 1) / PART_TILE + nodes;
+  return (unsigned)std::min<size_t>(tiles, (size_t)ctx->num_sms * 8);
+}
+
+// Blocks of a k_assign launch: one per class tree, and no more than 1024
+// threads in all when per-node sampling gives every thread a scratch row.
+static unsigned assign_blocks(const sb_booster* b, unsigned threads) {
+  const unsigned k = (unsigned)b->K;
+  return b->S.samp_scratch ? std::max(1u, std::min(k, 1024u / threads)) : k;
+}
+
 int booster_round_body(sb_booster* b, int apply_delta) {
   sb_ctx* ctx = b->ctx;
   BState& S = b->S;
@@ -2173,6 +2219,7 @@ int booster_round_body(sb_booster* b, int apply_delta) {
   L.ntiles = (int)b->g->tiles.size();
   L.rows_done = b->timing ? b->d_hist_rows.p : nullptr;
   L.pool_mask = S.pool_mask;
+  L.rows_bound = b->n * (size_t)b->K;  // each class tree's rows at most once per level
   const size_t esm = eval_smem(b);
   auto hist = [&](int max_items) -> int {
     L.max_items = max_items;
@@ -2206,10 +2253,11 @@ int booster_round_body(sb_booster* b, int apply_delta) {
     };
     SB_TRY(eval(0, 1));  // the root
     SB_LAUNCH(ctx, k_lg_heap, (unsigned)b->K, 256, heap_smem, S, 1);
-    const unsigned pblocks = (unsigned)ctx->num_sms * 8;
+    // a step partitions one node per class tree: its tiles, at most
+    const unsigned pblocks = part_blocks(ctx, b->n, b->K, b->K);
     for (int step = 0; step < b->steps; ++step) {
       const int d = step == 0 ? 0 : 1;  // only the first expansion reads the shared root list
-      SB_LAUNCH(ctx, k_assign, 1, 1024, 0, S, d, 1);
+      SB_LAUNCH(ctx, k_assign, assign_blocks(b, 128), 128, 0, S, d, 1);  // one frontier node per tree
       SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
       SB_LAUNCH(ctx, k_lg_copy, pblocks, 256, 0, S);
       SB_LAUNCH(ctx, k_plan, 1, 1024, 0, S, d);
@@ -2226,8 +2274,9 @@ int booster_round_body(sb_booster* b, int apply_delta) {
     SB_LAUNCH(ctx, k_eval_records, sg, EVAL_THREADS, esm, S, d);
     dim3 pg((width + SCAN_WARPS - 1) / SCAN_WARPS, (unsigned)b->K);
     SB_LAUNCH(ctx, k_eval_pick, pg, EVAL_THREADS, esm, S, d);
-    SB_LAUNCH(ctx, k_assign, 1, 1024, 0, S, d, 1);
-    unsigned pblocks = (unsigned)ctx->num_sms * 8;
+    const unsigned athreads = std::min(1024u, std::max(128u, width));
+    SB_LAUNCH(ctx, k_assign, assign_blocks(b, athreads), athreads, 0, S, d, 1);
+    const unsigned pblocks = part_blocks(ctx, b->n, b->K, (size_t)b->K * width);
     SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
     if (d + 1 < b->D) {
       SB_LAUNCH(ctx, k_plan, 1, 1024, 0, S, d);

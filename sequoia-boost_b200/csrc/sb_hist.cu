@@ -5,12 +5,13 @@
 //
 // Design: a persistent grid (one CTA of 1024 threads per SM) splits the
 // concatenated rows of every node to build (all frontier nodes of all class
-// trees in one launch) evenly over CTAs. A CTA keeps one node's histogram for
-// one feature tile in shared memory, walks its rows eight per warp (lanes 0-7
-// load the row ids one batch ahead and the gradient pairs, shuffles hand them
-// to the warp), adds every code of a row into the shared partial, and flushes
-// the non-zero entries to the node's HBM histogram with global atomics when it
-// moves to the next piece.
+// trees in one launch) evenly over CTAs (fewer CTAs for a launch known to
+// hold few rows). A CTA keeps one node's histogram for one feature tile in
+// shared memory, walks its rows in small batches per warp (the low lanes load
+// the row ids ahead and the gradient pairs, shuffles hand them to the warp;
+// TILED keeps two batches in flight), adds every code of a row into the
+// shared partial, and flushes the non-zero entries to the node's HBM
+// histogram with global atomics when it moves to the next piece.
 //   codes  TILED layout: lane l reads features 4l..4l+3 of the tile (one
 //          8-byte load per row) and a code is the entry's index in the tile's
 //          partial, where a feature's bins are contiguous. LANES layout: each
@@ -37,7 +38,8 @@ namespace {
 
 constexpr int HIST_THREADS = 1024;
 constexpr int MAX_TILE_FEATURES = 128;  // 4 features per lane
-constexpr int ROWS_PER_WARP = 8;        // rows in flight per warp
+constexpr int ROWS_PER_WARP = 8;        // LANES: rows per warp batch
+constexpr int TILED_ROWS = 4;           // TILED: rows per warp batch (two batches in flight)
 
 struct HistDev {
   const uint16_t* bins;
@@ -70,23 +72,7 @@ __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint
 
 // One addition into each plane of the shared partial, at the 32-bit shared
 // address `a` (g plane) and `a + hoff` (h plane), with `red` (no value
-// returned), only in the lanes where `on` holds: a predicate on the two
-// instructions rather than a branch around them. FIXED: int32 g and uint32
-// h; FP32: f32 bits.
-template <bool FIXED>
-__device__ __forceinline__ void add_pair_if(bool on, unsigned a, unsigned hoff, uint32_t vg, uint32_t vh) {
-  if (FIXED)
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %0, 0;\n\t"
-        "@p red.shared.add.s32 [%1], %2;\n\t@p red.shared.add.u32 [%3], %4;\n\t}" ::"r"((unsigned)on),
-        "r"(a), "r"(vg), "r"(a + hoff), "r"(vh));
-  else
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %0, 0;\n\t"
-        "@p red.shared.add.f32 [%1], %2;\n\t@p red.shared.add.f32 [%3], %4;\n\t}" ::"r"((unsigned)on),
-        "r"(a), "f"(__uint_as_float(vg)), "r"(a + hoff), "f"(__uint_as_float(vh)));
-}
-
+// returned). FIXED: int32 g and uint32 h; FP32: f32 bits.
 template <bool FIXED>
 __device__ __forceinline__ void add_pair(unsigned a, unsigned hoff, uint32_t vg, uint32_t vh) {
   if (FIXED) {
@@ -158,66 +144,89 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     }
     __syncthreads();
 
-    // Lane q < ROWS_PER_WARP holds row q of the warp's batch: its row id
-    // (loaded one batch ahead) and its gradient pair; the other lanes get them
-    // by shuffles. Every lane then loads its 4 codes of each row.
+    // Rows go through a warp in batches of TILED_ROWS, double-buffered: the
+    // codes and gradient pairs of the next batch are loaded before the adds of
+    // the current one, so the gather is in flight while the shared atomics
+    // issue. Lane q < TILED_ROWS holds row q of a batch (its id, loaded two
+    // batches ahead, and its gradient pair); the other lanes get them by
+    // shuffles. Every lane loads its 4 codes of each row.
     double tg = 0.0, th = 0.0;
     long long tqg = 0;
     unsigned long long tqh = 0;
     unsigned int nsampled = 0;
     const size_t gcol = (size_t)item.k * a.n;
     const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
-    const uint32_t stride = (uint32_t)nwarps * ROWS_PER_WARP;
-    uint32_t p = pbeg + warp * ROWS_PER_WARP;
-    uint32_t next_rid = 0u;
-    if (lane < ROWS_PER_WARP && p + lane < pend) next_rid = item.rows[p + lane];
-    for (; p < pend; p += stride) {
-      const uint32_t my_rid = next_rid;
-      const uint32_t pn = p + stride + lane;
-      next_rid = (lane < ROWS_PER_WARP && pn < pend) ? item.rows[pn] : 0u;
-      // rows of this batch (the lists hold sampled rows only), the same in every lane
-      const uint32_t nrow = min(pend - p, (uint32_t)ROWS_PER_WARP);
-      uint32_t my_g = 0u, my_h = 0u;  // FIXED ints or FP32 float bits
-      if (lane < (int)nrow) {
+    constexpr int R = TILED_ROWS;
+    const uint32_t stride = (uint32_t)nwarps * R;
+    // the gradient pair of the batch at p (lanes < its rows), counted into the totals
+    auto load_grad = [&](uint32_t rid, uint32_t nr, uint32_t& g, uint32_t& h) {
+      g = 0u;
+      h = 0u;
+      if (lane < (int)nr) {
         if (FIXED) {
-          const unsigned long long pk = reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + my_rid];
-          my_g = (uint32_t)(pk >> 32);
-          my_h = (uint32_t)(pk & 0xFFFFFFFFull);
+          const unsigned long long pk = reinterpret_cast<const unsigned long long*>(a.gpair)[gcol + rid];
+          g = (uint32_t)(pk >> 32);
+          h = (uint32_t)(pk & 0xFFFFFFFFull);
         } else {
-          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + my_rid];
-          my_g = __float_as_uint(v.x);
-          my_h = __float_as_uint(v.y);
+          const float2 v = reinterpret_cast<const float2*>(a.gpair)[gcol + rid];
+          g = __float_as_uint(v.x);
+          h = __float_as_uint(v.y);
         }
         nsampled++;
         if (want_total) {
           if (FIXED) {
-            tqg += (int)my_g;
-            tqh += my_h;
+            tqg += (int)g;
+            tqh += h;
           } else {
-            tg += (double)__uint_as_float(my_g);
-            th += (double)__uint_as_float(my_h);
+            tg += (double)__uint_as_float(g);
+            th += (double)__uint_as_float(h);
           }
         }
       }
-      uint2 bv[ROWS_PER_WARP];
+    };
+    // the codes of the batch's rows (the lists hold sampled rows only)
+    auto load_codes = [&](uint32_t rid, uint32_t nr, uint2 (&bv)[R]) {
 #pragma unroll
-      for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const uint32_t id = __shfl_sync(0xFFFFFFFFu, my_rid, q);
-        bv[q] = ((uint32_t)q < nrow && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + id * a.Fp))
-                                                : make_uint2(0u, 0u);
+      for (int q = 0; q < R; ++q) {
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, rid, q);
+        bv[q] = ((uint32_t)q < nr && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + (size_t)id * a.Fp))
+                                              : make_uint2(0u, 0u);
       }
+    };
+    uint32_t p = pbeg + warp * R;
+    uint32_t rid_c = (lane < R && p + lane < pend) ? item.rows[p + lane] : 0u;
+    uint32_t nrow_c = p < pend ? min(pend - p, (uint32_t)R) : 0u;
+    uint32_t g_c, h_c;
+    uint2 bv_c[R];
+    load_grad(rid_c, nrow_c, g_c, h_c);
+    load_codes(rid_c, nrow_c, bv_c);
+    uint32_t rid_n = (lane < R && p + stride + lane < pend) ? item.rows[p + stride + lane] : 0u;
+    for (; p < pend; p += stride) {
+      const uint32_t pn = p + stride;
+      const uint32_t nrow_n = pn < pend ? min(pend - pn, (uint32_t)R) : 0u;
+      uint32_t g_n, h_n;
+      uint2 bv_n[R];
+      load_grad(rid_n, nrow_n, g_n, h_n);
+      load_codes(rid_n, nrow_n, bv_n);
+      const uint32_t rid_nn = (lane < R && pn + stride + lane < pend) ? item.rows[pn + stride + lane] : 0u;
 #pragma unroll
-      for (int q = 0; q < ROWS_PER_WARP; ++q) {
-        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, my_g, q);
-        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, my_h, q);
-        if ((uint32_t)q >= nrow) break;
+      for (int q = 0; q < R; ++q) {
+        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, g_c, q);
+        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, h_c, q);
+        if ((uint32_t)q >= nrow_c) break;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const uint32_t w = j < 2 ? bv[q].x : bv[q].y;
+          const uint32_t w = j < 2 ? bv_c[q].x : bv_c[q].y;
           const unsigned idx = (j & 1) ? (w >> 16) : (w & 0xFFFFu);  // the tile-relative code
-          add_pair_if<FIXED>(fon[j], sh_base + 4u * idx, hoff, vg, vh);
+          if (fon[j]) add_pair<FIXED>(sh_base + 4u * idx, hoff, vg, vh);
         }
       }
+      g_c = g_n;
+      h_c = h_n;
+      nrow_c = nrow_n;
+      rid_n = rid_nn;
+#pragma unroll
+      for (int q = 0; q < R; ++q) bv_c[q] = bv_n[q];
     }
     if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
     if (want_total && lane < ROWS_PER_WARP) {
@@ -392,7 +401,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_lanes(HistDev a) {
         if ((uint32_t)q >= nrow) break;
 #pragma unroll
         for (int s = 0; s < S; ++s)
-          add_pair_if<FIXED>(fon[s], sh_base + 4u * (unsigned)(C::get(cv[q], s) * 32 + lane), hoff, vg, vh);
+          if (fon[s]) add_pair<FIXED>(sh_base + 4u * (unsigned)(C::get(cv[q], s) * 32 + lane), hoff, vg, vh);
       }
     }
     if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
@@ -711,12 +720,20 @@ const void* hist_kernel(const Ghist* g, bool fixed) {
 
 }  // namespace
 
-int hist_grid(sb_ctx* ctx, const Ghist* g) {
+// The persistent grid: every resident CTA, or for a launch known to hold
+// few rows one CTA per HIST_MIN_ROWS_PER_CTA (row, tile) units, so that a
+// small job's launch zeroes and flushes few shared partials and leaves SMs
+// to the launches of other streams.
+constexpr size_t HIST_MIN_ROWS_PER_CTA = 4096;
+int hist_grid(sb_ctx* ctx, const Ghist* g, size_t rows_bound) {
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_kernel(g, true), HIST_THREADS,
                                                 g->hist_smem_bytes);
   if (per_sm < 1) per_sm = 1;
-  return ctx->num_sms * per_sm;
+  const size_t full = (size_t)ctx->num_sms * per_sm;
+  if (rows_bound == 0) return (int)full;
+  const size_t want = (rows_bound * g->tiles.size() + HIST_MIN_ROWS_PER_CTA - 1) / HIST_MIN_ROWS_PER_CTA;
+  return (int)std::max<size_t>(1, std::min(full, want));
 }
 
 int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
@@ -738,7 +755,7 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.rows_done = L.rows_done;
   a.pool_mask = L.pool_mask;
   a.FW = (int)((L.g->F + 31) / 32);
-  const int grid = hist_grid(ctx, L.g);
+  const int grid = hist_grid(ctx, L.g, L.rows_bound);
   const size_t sm = L.g->hist_smem_bytes;
   void (*kern)(HistDev) = L.fixed ? k_hist<true> : k_hist<false>;
   if (L.g->layout == HIST_LAYOUT_LANES) {

@@ -215,6 +215,7 @@ struct HistLaunch {
   int ntiles;
   unsigned long long* rows_done;  // device counter of sampled rows, or null
   const uint32_t* pool_mask;      // device [K][ceil(F/32)]: features to accumulate, or null
+  size_t rows_bound = 0;          // most rows one launch accumulates (0: unknown, full grid)
 };
 
 // One layout of the histogram's bin codes (HIST_LAYOUT_*; LANES: positions
@@ -230,7 +231,7 @@ int hist_time(sb_ctx* ctx, const Ghist* g, float* ms);
 int launch_hist(sb_ctx* ctx, const HistLaunch& L);
 int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const int* count,
                       int max_items);
-int hist_grid(sb_ctx* ctx, const Ghist* g);
+int hist_grid(sb_ctx* ctx, const Ghist* g, size_t rows_bound);
 
 // ----------------------------------------------------------------- model
 struct HostTree {

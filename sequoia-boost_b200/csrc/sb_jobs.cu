@@ -2,13 +2,14 @@
 // parameter sweeps) of uneven sizes trained together on one GPU.
 //
 // Each job gets its own binned matrix and device booster (train(), learner/
-// train.rs:107-113, per job). Jobs are spread round-robin over a pool of
-// streams; the host then issues round r of every unfinished job before
+// train.rs:107-113, per job), set up by a few host threads at once. Jobs are
+// spread round-robin over a pool of streams; the host then issues round r of every unfinished job before
 // round r + 1 of any, so the GPU always holds work of many jobs at once and
 // small jobs fill the SMs that one small job alone would leave idle. From its
 // third round on, a job's round is one CUDA-graph launch, so issuing a round
 // of every job costs the host a few microseconds per job.
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "sb_internal.cuh"
@@ -32,15 +33,30 @@ int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams) {
   std::vector<sb_booster*> bo(n_jobs, nullptr);
   int rc = SB_OK;
   for (int s = 0; s < S && rc == SB_OK; ++s) rc = sb_ctx_create(ctx->device, &sctx[s]);
-  // set-up: bin each job's matrix and create its booster on its stream
-  for (size_t j = 0; j < n_jobs && rc == SB_OK; ++j) {
-    sb_job& jb = jobs[j];
-    sb_ctx* c = sctx[j % S];
-    int s = sb_train_params_validate(jb.params);
-    if (s == SB_OK)
-      s = sb_ghist_create(c, jb.X, jb.n_rows, jb.n_cols, jb.feature_types, jb.missing, jb.params->max_bin, &gh[j]);
-    if (s == SB_OK) s = sb_booster_create(c, gh[j], jb.params, jb.labels, jb.weights, jb.base_margin, &bo[j]);
-    jb.status = s;
+  // set-up: bin each job's matrix and create its booster on its stream.
+  // Binning waits for its cuts on the host, so host threads set up jobs in
+  // parallel: thread t takes the streams s with s % T == t (a stream's jobs
+  // stay on one thread).
+  if (rc == SB_OK) {
+    const int T = std::max(1, std::min(S, (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency()))));
+    auto setup = [&](int t) {
+      cudaSetDevice(ctx->device);
+      for (size_t j = 0; j < n_jobs; ++j) {
+        if ((int)(j % S) % T != t) continue;
+        sb_job& jb = jobs[j];
+        sb_ctx* c = sctx[j % S];
+        int s = sb_train_params_validate(jb.params);
+        if (s == SB_OK)
+          s = sb_ghist_create(c, jb.X, jb.n_rows, jb.n_cols, jb.feature_types, jb.missing, jb.params->max_bin,
+                              &gh[j]);
+        if (s == SB_OK) s = sb_booster_create(c, gh[j], jb.params, jb.labels, jb.weights, jb.base_margin, &bo[j]);
+        jb.status = s;
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(setup, t);
+    setup(0);
+    for (std::thread& th : pool) th.join();
   }
   // rounds, interleaved across jobs
   int max_rounds = 0;
