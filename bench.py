@@ -405,12 +405,12 @@ def c3_leg(sb, ctx, args):
              sb.DMatrix(j["x"], labels=j["y"]), 100) for j in jobs]
     sb.train_many(spec[:4], ctx=ctx)  # warm-up
     t0 = time.perf_counter()
-    models = sb.train_many(spec, n_streams=16, ctx=ctx)
+    models = sb.train_many(spec, n_streams=32, ctx=ctx)
     t = time.perf_counter() - t0
     rows = sum(j["x"].shape[0] for j in jobs)
     assert all(m is not None for m in models)
     return {"workload": f"{len(jobs)} regression jobs, {rows} rows in total, 20-50 features, 100 rounds each, "
-                        "max_bin 64, one sb_train_many call (16 streams)",
+                        "max_bin 64, one sb_train_many call (32 streams)",
             "value": rows * 100 / t / 1e6, "unit": UNIT, "seconds": t}
 
 

@@ -830,7 +830,7 @@ class EarlyStopping:
         return False
 
 
-def train_many(jobs, n_streams=16, ctx: Context = None):
+def train_many(jobs, n_streams=32, ctx: Context = None):
     """Trains independent jobs together on the GPU (sb_train_many): `jobs` is
     a list of (TrainingParams, DMatrix with labels, num_boost_round). Returns
     one BoostedModel per job, each equal to what `train` gives for that job."""

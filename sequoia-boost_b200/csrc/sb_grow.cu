@@ -65,6 +65,7 @@ struct HeapEnt {
 struct BState {
   // shapes
   int K, F, FW, HB, total_bins, max_depth, maxn, maxw, cat_cap;
+  int cat_bins;             // most bins of a categorical feature (eval scratch entries)
   // lossguide growth (grow_lossguide, hist.rs:238-268)
   int lossguide;
   int max_leaves;           // leaf budget (2^max_depth when max_leaves is 0)
@@ -656,13 +657,31 @@ __device__ __forceinline__ double warp_excl_max(double v, double init) {
 }
 
 // Scratch of one warp for a categorical feature.
+// One warp's categorical scratch: arrays of `cap` entries (the most bins of
+// a categorical feature of the index), carved from the block's dynamic
+// shared memory so that the eval kernels' occupancy follows the data.
 struct CatScratch {
-  double g[MAX_CAT_BINS];
-  double h[MAX_CAT_BINS];
-  long long key[MAX_CAT_BINS];
-  uint16_t ne[MAX_CAT_BINS];      // non-empty bins, ascending
-  uint16_t order[MAX_CAT_BINS];   // positions into ne/g/h, sorted by ratio (stable)
+  double* g;
+  double* h;
+  long long* key;
+  uint16_t* ne;      // non-empty bins, ascending
+  uint16_t* order;   // positions into ne/g/h, sorted by ratio (stable)
 };
+
+__host__ __device__ constexpr size_t cat_scratch_bytes(int cap) {
+  return ((size_t)cap * (8 + 8 + 8 + 2 + 2) + 7) / 8 * 8;
+}
+
+__device__ __forceinline__ CatScratch cat_scratch(double* base, int warp, int cap) {
+  double* b = base + (size_t)warp * (cat_scratch_bytes(cap) / 8);
+  CatScratch c;
+  c.g = b;
+  c.h = b + cap;
+  c.key = reinterpret_cast<long long*>(b + 2 * cap);
+  c.ne = reinterpret_cast<uint16_t*>(b + 3 * cap);
+  c.order = c.ne + cap;
+  return c;
+}
 
 constexpr int AMB_MAX = 6;  // ambiguous records kept per (node, feature)
 
@@ -962,7 +981,9 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) {
   double m = -INFINITY;
   if (in_mask(S.fmask + ni * S.FW, f)) {
     const EvalNode E = eval_node(S, k, ni, d);
-    CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+    CatScratch csv{};
+  if (S.cat_cap > 0) csv = cat_scratch(ev_sm, warp, S.cat_bins);
+  CatScratch* cs = S.cat_cap > 0 ? &csv : nullptr;
     m = scan_feature<SCAN_MAX>(S, H, k, f, E, 0.0, cs, nullptr, nullptr).gain;
   }
   if (lane == 0) S.mbuf[((size_t)k * S.maxw + slot) * S.F + f] = m;
@@ -998,7 +1019,9 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) 
     if (in_mask(fm, j)) q = fmax(q, M[j]);
   q = warp_max(q);
   const EvalNode E = eval_node(S, k, ni, d);
-  CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+  CatScratch csv{};
+  if (S.cat_cap > 0) csv = cat_scratch(ev_sm, warp, S.cat_bins);
+  CatScratch* cs = S.cat_cap > 0 ? &csv : nullptr;
   scan_feature<SCAN_RECORDS>(S, frontier_hist(S, d, k, slot), k, f, E, q, cs, s_gains[warp], nullptr, rec);
 }
 
@@ -1020,7 +1043,9 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
   const double* M = S.mbuf + ((size_t)k * S.maxw + slot) * S.F;
   const FeatRec* R = S.frec + ((size_t)k * S.maxw + slot) * S.F;
   const uint32_t* fm = S.fmask + ni * S.FW;
-  CatScratch* cs = S.cat_cap > 0 ? reinterpret_cast<CatScratch*>(ev_sm) + warp : nullptr;
+  CatScratch csv{};
+  if (S.cat_cap > 0) csv = cat_scratch(ev_sm, warp, S.cat_bins);
+  CatScratch* cs = S.cat_cap > 0 ? &csv : nullptr;
   // last feature holding a certain record
   int fstar = -1;
   for (int j = lane; j < S.F; j += 32)
@@ -2079,6 +2104,9 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.n_leaves = b->d_heap_size.p ? b->d_heap_size.p + K : nullptr;
   S.ndepth = b->d_ndepth.p;
   S.cat_cap = g->has_categorical ? (b->maxn / 2 + 1) * g->max_feature_bins : 0;
+  S.cat_bins = 1;
+  for (size_t f = 0; f < g->F; ++f)
+    if (g->h_is_cat[f]) S.cat_bins = std::max(S.cat_bins, (int)(g->h_foff[f + 1] - g->h_foff[f]));
   S.n = b->n;
   S.Fp = g->Fp;
   S.bins = g->bins.p;
@@ -2168,7 +2196,7 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
 }
 
 size_t eval_smem(const sb_booster* b) {
-  return b->S.cat_cap ? (EVAL_THREADS / 32) * sizeof(CatScratch) : 0;
+  return b->S.cat_cap ? (EVAL_THREADS / 32) * cat_scratch_bytes(b->S.cat_bins) : 0;
 }
 
 // The launches of one boosting round on the context stream (also recorded into

@@ -273,6 +273,7 @@ struct DevEnsemble {
   DBuf<float> shap_tab;      // per path: [2^D][round_up(D, 4)] f32 contributions
   DBuf<long long> shap_tab_off;  // [n_paths] first float of each path's table
   DBuf<int4> tab_el;         // per element: {feature, lo, hi, (table-chunk feature index << 1) | miss_ok}
+  DBuf<int4> tab_head;       // per path: {first element, elements, table offset low, high 32 bits}
   DBuf<int4> tab_chunk;      // {class, first tree, trees, -}: work units of the table kernel
   DBuf<int> tab_chunk_fo;    // [n_tab_chunks + 1] offsets into tab_chunk_f
   DBuf<int> tab_chunk_f;     // each table chunk's distinct features

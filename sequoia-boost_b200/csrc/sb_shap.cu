@@ -487,6 +487,8 @@ constexpr int TAB_ROWS = 64;
 constexpr int TAB_STRIDE = TAB_ROWS + 1;  // words per feature in the row-value copy
 constexpr int TAB_CHUNK_PATHS = 1024;
 constexpr int TAB_CHUNK_FEATURES = 192;  // distinct features of a chunk (its partial's rows)
+constexpr int TAB_TPR = 8;               // threads per row
+constexpr int TAB_ILP = 1;               // paths in flight per thread
 
 // Shared memory of one k_shap_table block for a chunk of `nfc` features:
 // the f32 partials [nfc][TAB_ROWS] and the row values [nfc][TAB_STRIDE].
@@ -496,8 +498,7 @@ __host__ __device__ constexpr size_t shap_table_smem(int nfc) {
 
 struct ShapTabDev {
   const int4* el;           // per element: {feature, lo bits, hi bits, (chunk feature index << 1) | miss_ok}
-  const int* off;           // [n_paths + 1] element offsets (element 0 of a path is its bias)
-  const long long* tab_off; // per path: first float of its table
+  const int4* head;         // per path: {first element, elements, table offset (two 32-bit halves)}
   const float* tab;
   const int* tree_path;     // [n_trees + 1]
   const int4* chunk;        // {class, first tree, number of trees, -}; trees t, t + K, t + 2K, ...
@@ -506,12 +507,14 @@ struct ShapTabDev {
   int K;
 };
 
-__global__ void __launch_bounds__(TAB_ROWS) k_shap_table(ShapTabDev P, const float* __restrict__ X, size_t n,
-                                                        int F, float missing, unsigned row_blocks,
-                                                        double* __restrict__ acc) {
+template <int TPR, int ILP>
+__global__ void __launch_bounds__(TAB_ROWS * TPR, 1024 / (TAB_ROWS * TPR))
+k_shap_table(ShapTabDev P, const float* __restrict__ X, size_t n, int F, float missing, unsigned row_blocks,
+             double* __restrict__ acc) {
   extern __shared__ float ph[];  // [chunk features][TAB_ROWS], then xs
   const int R = TAB_ROWS;
   const int tid = threadIdx.x;
+  const int row = tid % R, grp = tid / R;  // a row's TPR threads take every TPR-th group of paths
   const unsigned rb = blockIdx.x % row_blocks;
   const size_t r0 = (size_t)rb * R;
   const unsigned ci = blockIdx.x / row_blocks;
@@ -519,32 +522,40 @@ __global__ void __launch_bounds__(TAB_ROWS) k_shap_table(ShapTabDev P, const flo
   const int c = ch.x;
   const int fo = P.chunk_fo[ci], nfc = P.chunk_fo[ci + 1] - fo;
   float* xs = ph + (size_t)nfc * R;  // [chunk features][TAB_STRIDE] row values
-  for (int i = tid; i < nfc * R; i += R) ph[i] = 0.0f;
+  for (int i = tid; i < nfc * R; i += blockDim.x) ph[i] = 0.0f;
   // consecutive threads read consecutive chunk features of one row
   const int rows_here = (int)min((size_t)R, n - r0);
-  for (int i = tid; i < nfc * rows_here; i += R) {
+  for (int i = tid; i < nfc * rows_here; i += blockDim.x) {
     const int r = i / nfc, j = i - r * nfc;
     xs[j * TAB_STRIDE + r] = __ldg(X + (r0 + r) * (size_t)F + P.chunk_f[fo + j]);
   }
   __syncthreads();
   const bool miss_nan = isnan(missing);
-  const float* xr = xs + tid;
+  const float* xr = xs + row;
+  float* pr = ph + row;
   for (int ti = 0; ti < ch.z; ++ti) {
     const int t = ch.y + ti * P.K;
     const int pe = P.tree_path[t + 1];
-    for (int p0 = P.tree_path[t]; p0 < pe; p0 += 4) {
-      unsigned m[4];
-      int eb[4], dn[4];
+    for (int p0 = P.tree_path[t] + grp * ILP; p0 < pe; p0 += TPR * ILP) {
+      // ILP paths at a time, every element loop unrolled to the table depth
+      // limit, so that all their element and table loads are in flight
+      // together; each element's chunk-feature index stays in a register for
+      // the partial updates.
+      int4 hd[ILP];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {  // patterns
-        m[u] = 0u;
-        eb[u] = 0;
-        dn[u] = 0;
-        if (p0 + u < pe) {
-          eb[u] = P.off[p0 + u] + 1;
-          dn[u] = P.off[p0 + u + 1] - eb[u];
-          for (int e = 0; e < dn[u]; ++e) {
-            const int4 x = __ldg(P.el + eb[u] + e);
+      for (int u = 0; u < ILP; ++u) hd[u] = p0 + u < pe ? __ldg(P.head + p0 + u) : make_int4(0, 0, 0, 0);
+      unsigned m[ILP];
+      int fc[ILP][SHAP_TABLE_MAXD];
+#pragma unroll
+      for (int u = 0; u < ILP; ++u) m[u] = 0u;
+#pragma unroll
+      for (int e = 0; e < SHAP_TABLE_MAXD; ++e) {
+#pragma unroll
+        for (int u = 0; u < ILP; ++u) {
+          fc[u][e] = 0;
+          if (e < hd[u].y) {
+            const int4 x = __ldg(P.el + hd[u].x + e);
+            fc[u][e] = x.w >> 1;
             const float v = xr[(x.w >> 1) * TAB_STRIDE];
             const bool mis = miss_nan ? isnan(v) : v == missing;
             const bool o = mis ? (x.w & 1) != 0 : (v >= __int_as_float(x.y) && v < __int_as_float(x.z));
@@ -552,32 +563,36 @@ __global__ void __launch_bounds__(TAB_ROWS) k_shap_table(ShapTabDev P, const flo
           }
         }
       }
-      float4 tv[4][3];
+      float4 tv[ILP][3];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {  // the table entries of the four patterns
-        const int dp = (dn[u] + 3) & ~3;
-        const float4* t4 = reinterpret_cast<const float4*>(P.tab + P.tab_off[p0 + u < pe ? p0 + u : p0] +
-                                                           (long long)m[u] * dp);
+      for (int u = 0; u < ILP; ++u) {  // the table entries of the patterns
+        const int dn = hd[u].y, dp = (dn + 3) & ~3;
+        const long long toff = (long long)(((unsigned long long)(uint32_t)hd[u].w << 32) | (uint32_t)hd[u].z);
+        const float4* t4 = reinterpret_cast<const float4*>(P.tab + toff + (long long)m[u] * dp);
 #pragma unroll
-        for (int j = 0; j < 3; ++j) tv[u][j] = 4 * j < dn[u] ? __ldg(t4 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < 3; ++j) tv[u][j] = 4 * j < dn ? __ldg(t4 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < ILP; ++u) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const float vv[4] = {tv[u][j].x, tv[u][j].y, tv[u][j].z, tv[u][j].w};
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (4 * j + q < dn[u]) ph[(__ldg(&P.el[eb[u] + 4 * j + q].w) >> 1) * R + tid] += vv[q];
+            if (4 * j + q < SHAP_TABLE_MAXD && 4 * j + q < hd[u].y) {
+              if (TPR == 1) pr[fc[u][4 * j + q] * R] += vv[q];
+              else atomicAdd(pr + fc[u][4 * j + q] * R, vv[q]);  // the row's other threads add too
+            }
         }
       }
     }
   }
-  if (r0 + tid < n) {
+  __syncthreads();
+  if (r0 + row < n) {
     const int Kc = P.K;
-    double* a = acc + ((r0 + tid) * Kc + c) * (size_t)(F + 1);
-    for (int j = 0; j < nfc; ++j) {
-      const float v = ph[j * R + tid];
+    double* a = acc + ((r0 + row) * Kc + c) * (size_t)(F + 1);
+    for (int j = grp; j < nfc; j += TPR) {
+      const float v = ph[j * R + row];
       if (v != 0.0f) atomicAdd(a + P.chunk_f[fo + j], (double)v);
     }
   }
@@ -878,6 +893,12 @@ int shap_prepare(sb_model* m) {
           tfo.push_back((int)tf.size());
         }
       }
+      std::vector<int4> thead(n_paths);
+      for (int p = 0; p < n_paths; ++p)
+        thead[p] = make_int4(poff[p] + 1, poff[p + 1] - poff[p] - 1, (int)(uint32_t)(toff[p] & 0xFFFFFFFFll),
+                             (int)(toff[p] >> 32));
+      SB_TRY(D.tab_head.alloc(ctx, std::max(n_paths, 1)));
+      SB_CUDA(cudaMemcpyAsync(D.tab_head.p, thead.data(), n_paths * 16, cudaMemcpyHostToDevice, st));
       SB_TRY(D.tab_el.alloc(ctx, std::max<size_t>(tel.size(), 1)));
       SB_TRY(D.tab_chunk.alloc(ctx, std::max<size_t>(tch.size(), 1)));
       SB_TRY(D.tab_chunk_fo.alloc(ctx, tfo.size()));
@@ -891,7 +912,7 @@ int shap_prepare(sb_model* m) {
       // a tree with more distinct features than one block's partial can hold
       // keeps the f64 path kernels
       if (shap_table_smem(tmax) <= ctx->smem_optin) {
-        SB_TRY(raise_smem_limit((const void*)k_shap_table, shap_table_smem(tmax)));
+        SB_TRY(raise_smem_limit((const void*)k_shap_table<TAB_TPR, TAB_ILP>, shap_table_smem(tmax)));
         D.shap_table = true;
       }
       SB_CUDA(cudaStreamSynchronize(st));  // d_moff and the host vectors are released on return
@@ -951,8 +972,7 @@ int shap_paths(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t 
   if (m->dev.shap_table) {
     ShapTabDev Q;
     Q.el = m->dev.tab_el.p;
-    Q.off = m->dev.path_off.p;
-    Q.tab_off = m->dev.shap_tab_off.p;
+    Q.head = m->dev.tab_head.p;
     Q.tab = m->dev.shap_tab.p;
     Q.tree_path = m->dev.tree_path.p;
     Q.chunk = m->dev.tab_chunk.p;
@@ -962,7 +982,8 @@ int shap_paths(sb_model* m, cudaStream_t st, const float* d_X, size_t n, size_t 
     const unsigned trb = (unsigned)((n + TAB_ROWS - 1) / TAB_ROWS);
     const unsigned long long tb = (unsigned long long)trb * (unsigned long long)m->dev.n_tab_chunks;
     SB_REQUIRE(tb < (1ull << 31), SB_ERR_UNSUPPORTED, "TreeSHAP of %zu rows exceeds one launch", n);
-    SB_LAUNCH_ON(ctx, st, k_shap_table, (unsigned)tb, TAB_ROWS, shap_table_smem(m->dev.tab_max_fc), Q, d_X, n,
+    SB_LAUNCH_ON(ctx, st, (k_shap_table<TAB_TPR, TAB_ILP>), (unsigned)tb, TAB_ROWS * TAB_TPR,
+                 shap_table_smem(m->dev.tab_max_fc), Q, d_X, n,
                  (int)F, missing, trb, d_acc);
   } else if (L <= 5) {
     SB_LAUNCH_ON(ctx, st, k_shap_paths<5>, grid, R, smem, P, d_X, n, (int)F, K, missing, row_blocks, d_acc);
