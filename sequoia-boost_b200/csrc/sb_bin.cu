@@ -620,7 +620,9 @@ int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_TRY(g->fmiss.alloc(ctx, F));
   SB_CUDA(cudaMemcpyAsync(g->fbase.p, zeros.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(g->fmiss.p, miss.data(), F * 4, cudaMemcpyHostToDevice, st));
-  DBuf<int> rpos, rbase, rmiss;
+  DBuf<int>& rpos = g->rpos;
+  DBuf<int>& rbase = g->rbase;
+  DBuf<int>& rmiss = g->rmiss;
   SB_TRY(rpos.alloc(ctx, F));
   SB_TRY(rbase.alloc(ctx, F));
   SB_TRY(rmiss.alloc(ctx, F));
@@ -634,7 +636,7 @@ int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
   const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 32);
   SB_LAUNCH(ctx, k_bin, blocks, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
             g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
-  SB_CUDA(cudaStreamSynchronize(st));  // temporaries and host vectors are released on return
+  SB_CUDA(cudaStreamSynchronize(st));  // the host vectors are released on return
   return SB_OK;
 }
 

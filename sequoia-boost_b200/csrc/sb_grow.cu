@@ -82,6 +82,9 @@ struct BState {
   const uint16_t* bins_col;  // the same, feature-major
   const int* fbase;          // code of local bin 0, per feature
   const int* fmiss;          // code of a missing entry, per feature
+  const int* rpos;           // row-major codes: position, code of local bin 0 and
+  const int* rbase;          // code of a missing entry of each feature
+  const int* rmiss;
   const uint32_t* foff;
   const float* cuts;
   const uint8_t* is_cat;
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(256) k_gradient(BState S) {
   const int K = S.K;
   const size_t n = S.n;
   for (int c = 0; c < 16; ++c) mg[c] = mh[c] = 0.0f;
-  __shared__ unsigned int s_cnt[2], s_base[2], s_wk[8], s_wu[8];
+  __shared__ unsigned int s_base[2], s_wk[8], s_wu[8];
   __shared__ unsigned int s_max[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const size_t per = (n + gridDim.x - 1) / gridDim.x;
@@ -296,25 +299,40 @@ __global__ void __launch_bounds__(256) k_gradient(BState S) {
     if (S.ext_gpair) return !(S.rows1[r] & UNSAMPLED);
     return S.subsample >= 1.0 || sb_u01(sb_row_draw(rk, r)) < S.subsample;
   };
+  // each warp owns a contiguous part of the block's rows; the block's kept
+  // rows go to the front of the root list and the others to its back, both in
+  // row order (warp parts in order, ascending within a part)
+  const int nw = blockDim.x >> 5;
+  const size_t wper = (hi - lo + nw - 1) / nw;
+  const size_t wlo = min(hi, lo + (size_t)warp * wper), whi = min(hi, wlo + wper);
   unsigned int c0 = 0;
-  for (size_t r = lo + tid; r < hi; r += blockDim.x) c0 += keep_of(r) ? 1u : 0u;
-  if (tid < 2) s_cnt[tid] = 0u;
-  if (tid < 32) s_max[tid] = 0u;
-  __syncthreads();
+  for (size_t r = wlo + lane; r < whi; r += 32) c0 += keep_of(r) ? 1u : 0u;
   for (int o = 16; o > 0; o >>= 1) c0 += __shfl_xor_sync(0xFFFFFFFFu, c0, o);
-  if (lane == 0 && c0) atomicAdd(&s_cnt[0], c0);
+  if (tid < 32) s_max[tid] = 0u;
+  if (lane == 0) {
+    s_wk[warp] = c0;
+    s_wu[warp] = (unsigned int)(whi - wlo) - c0;
+  }
   __syncthreads();
   if (tid == 0) {  // one atomic per block and counter (same-address atomics serialise)
-    s_base[0] = s_cnt[0] ? atomicAdd(S.kept, s_cnt[0]) : 0u;
-    const unsigned int un = (unsigned int)(hi - lo) - s_cnt[0];
-    s_base[1] = un ? atomicAdd(S.unkept, un) : 0u;
+    unsigned int tk = 0, tu = 0;
+    for (int w = 0; w < nw; ++w) {
+      tk += s_wk[w];
+      tu += s_wu[w];
+    }
+    s_base[0] = tk ? atomicAdd(S.kept, tk) : 0u;
+    s_base[1] = tu ? atomicAdd(S.unkept, tu) : 0u;
   }
   __syncthreads();
   unsigned int front = s_base[0], back = s_base[1];
+  for (int w = 0; w < warp; ++w) {
+    front += s_wk[w];
+    back += s_wu[w];
+  }
   const unsigned lt = (1u << lane) - 1u;
-  for (size_t base = lo; base < hi; base += blockDim.x) {  // the same trip count in every thread
-    const size_t r = base + tid;
-    const bool valid = r < hi;
+  for (size_t base = wlo; base < whi; base += 32) {  // the same trip count in every lane
+    const size_t r = base + lane;
+    const bool valid = r < whi;
     bool keep = false;
     if (valid) {
       if (!S.ext_gpair) {
@@ -340,25 +358,10 @@ __global__ void __launch_bounds__(256) k_gradient(BState S) {
       keep = keep_of(r);
     }
     const unsigned km = __ballot_sync(0xFFFFFFFFu, keep), um = __ballot_sync(0xFFFFFFFFu, valid && !keep);
-    if (lane == 0) {
-      s_wk[warp] = __popc(km);
-      s_wu[warp] = __popc(um);
-    }
-    __syncthreads();
-    unsigned int ko = 0, uo = 0, kt = 0, ut = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      if (w < warp) {
-        ko += s_wk[w];
-        uo += s_wu[w];
-      }
-      kt += s_wk[w];
-      ut += s_wu[w];
-    }
-    if (keep) S.rows0[front + ko + __popc(km & lt)] = (uint32_t)r;
-    else if (valid) S.rows0[n - 1 - (back + uo + __popc(um & lt))] = (uint32_t)r;
-    front += kt;
-    back += ut;
-    __syncthreads();  // s_wk / s_wu are rewritten by the next tile
+    if (keep) S.rows0[front + __popc(km & lt)] = (uint32_t)r;
+    else if (valid) S.rows0[n - 1 - (back + __popc(um & lt))] = (uint32_t)r;
+    front += __popc(km);
+    back += __popc(um);
   }
   if (S.fixed) {
     for (int c = 0; c < K && c < 16; ++c) {
@@ -1652,6 +1655,7 @@ __global__ void k_lg_finalize(BState S) {
     out[nid].leaf_value = lv;
     S.leafval[ni] = lv;
   }
+  if (!S.row_leaf) return;  // k_lg_route gives every row its leaf values
   const uint2 sg = S.seg[ni];
   const uint32_t* rows = S.rows0 + (nid == 0 ? 0 : (size_t)k * S.n);  // an unsplit root keeps the shared list
   for (uint32_t p = sg.x + threadIdx.x; p < sg.y; p += blockDim.x) {
@@ -1659,6 +1663,38 @@ __global__ void k_lg_finalize(BState S) {
     const uint32_t id = rv & ~UNSAMPLED;
     if (S.update_margin) S.delta[(size_t)id * S.K + k] = lv;
     if (S.row_leaf) S.row_leaf[id] = (rv & UNSAMPLED) ? -1 : nid;
+  }
+}
+
+// Every row's leaf value in each class tree of the round (the margin update,
+// train.rs:326-328), sampled or not: the row is routed through the finished
+// tree with its row-major codes, whose few sectors stay in cache for all K
+// trees, and its K values are stored together. This replaces per-leaf writes
+// scattered over the whole delta array (and routing the unsampled rows alone).
+// The decisions are the partition's: missing -> default direction,
+// categorical -> the node's category set, numeric -> local bin <= split bin.
+__global__ void k_lg_route(BState S) {
+  const unsigned long long round = *S.round;
+  const int K = S.K;
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < S.n; r += (size_t)gridDim.x * blockDim.x) {
+    const uint16_t* row = S.bins + r * S.Fp;
+    for (int k = 0; k < K; ++k) {
+      const sb_node* out = S.out_nodes + ((size_t)round * K + k) * S.maxn;
+      int nid = 0;
+      while (out[nid].left != -1) {
+        const NodeSplit& sp = S.split[NI(S, k, nid)];
+        const int f = sp.feature;
+        const int code = (int)row[S.rpos[f]];
+        bool go;
+        if (code == S.rmiss[f]) go = sp.default_left != 0;
+        else {
+          const int c = code - S.rbase[f];
+          go = sp.is_cat ? ((sp.cat_mask[c >> 5] >> (c & 31)) & 1u) != 0 : c <= sp.bin;
+        }
+        nid = go ? out[nid].left : out[nid].right;
+      }
+      S.delta[r * K + k] = S.leafval[NI(S, k, nid)];
+    }
   }
 }
 
@@ -2113,6 +2149,9 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
   S.bins_col = g->bins_col.p;
   S.fbase = g->fbase.p;
   S.fmiss = g->fmiss.p;
+  S.rpos = g->rpos.p;
+  S.rbase = g->rbase.p;
+  S.rmiss = g->rmiss.p;
   S.foff = g->foff.p;
   S.cuts = g->cuts.p;
   S.is_cat = g->is_cat.p;
@@ -2285,7 +2324,7 @@ int booster_round_body(sb_booster* b, int apply_delta) {
     const unsigned pblocks = part_blocks(ctx, b->n, b->K, b->K);
     for (int step = 0; step < b->steps; ++step) {
       const int d = step == 0 ? 0 : 1;  // only the first expansion reads the shared root list
-      SB_LAUNCH(ctx, k_assign, assign_blocks(b, 128), 128, 0, S, d, 1);  // one frontier node per tree
+      SB_LAUNCH(ctx, k_assign, assign_blocks(b, 256), 256, 0, S, d, 1);  // one frontier node per tree
       SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
       SB_LAUNCH(ctx, k_lg_copy, pblocks, 256, 0, S);
       SB_LAUNCH(ctx, k_plan, 1, 1024, 0, S, d);
@@ -2294,6 +2333,7 @@ int booster_round_body(sb_booster* b, int apply_delta) {
       SB_LAUNCH(ctx, k_lg_heap, (unsigned)b->K, 256, heap_smem, S, 0);
     }
     SB_LAUNCH(ctx, k_lg_finalize, dim3((unsigned)b->maxn, (unsigned)b->K), 256, 0, S);
+    if (!S.row_leaf && S.update_margin) SB_LAUNCH(ctx, k_lg_route, gblocks, 256, 0, S);
   }
   for (int d = 0; d < b->D && !b->lossguide; ++d) {
     const unsigned width = (unsigned)std::min(1 << d, b->maxw);
@@ -2302,8 +2342,9 @@ int booster_round_body(sb_booster* b, int apply_delta) {
     SB_LAUNCH(ctx, k_eval_records, sg, EVAL_THREADS, esm, S, d);
     dim3 pg((width + SCAN_WARPS - 1) / SCAN_WARPS, (unsigned)b->K);
     SB_LAUNCH(ctx, k_eval_pick, pg, EVAL_THREADS, esm, S, d);
-    const unsigned athreads = std::min(1024u, std::max(128u, width));
-    SB_LAUNCH(ctx, k_assign, assign_blocks(b, athreads), athreads, 0, S, d, 1);
+    // 1024 threads: the threads also write the level's partition tiles (about
+    // n / PART_TILE at the root), one binary search each
+    SB_LAUNCH(ctx, k_assign, assign_blocks(b, 1024), 1024, 0, S, d, 1);
     const unsigned pblocks = part_blocks(ctx, b->n, b->K, (size_t)b->K * width);
     SB_LAUNCH(ctx, k_partition, pblocks, PART_THREADS, 0, S, d);
     if (d + 1 < b->D) {
@@ -2311,8 +2352,9 @@ int booster_round_body(sb_booster* b, int apply_delta) {
       SB_TRY(hist(b->K * (1 << d)));
     }
   }
-  // the rows outside the subset take their leaf values by routing
-  SB_LAUNCH(ctx, k_route_rest, gblocks, 256, 0, S);
+  // the rows outside the subset take their leaf values by routing (lossguide
+  // rounds without row -> leaf output routed every row above)
+  if (!b->lossguide || S.row_leaf) SB_LAUNCH(ctx, k_route_rest, gblocks, 256, 0, S);
   SB_LAUNCH(ctx, k_round_end, 1, 32, 0, S);
   if (b->timing) {
     SB_CUDA(cudaEventRecord(r1, ctx->stream));

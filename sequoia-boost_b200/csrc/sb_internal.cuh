@@ -151,6 +151,7 @@ struct Ghist {  // sb_ghist
   // entry; unused positions hold 0xFFFF.
   DBuf<uint16_t> bins;
   std::vector<int> h_rpos, h_rbase, h_rmiss;
+  DBuf<int> rpos, rbase, rmiss;  // device copies of h_rpos, h_rbase, h_rmiss
   DBuf<int> ent_gbin;      // LANES: per tile, [E][32] histogram bin of each (entry, lane), -1 unused
   DBuf<int> slot_feat;     // LANES: [Fp] feature of each code position, -1 unused
   // [F][n] local bins, feature-major, MISSING_BIN for a missing entry (the

@@ -508,7 +508,7 @@ struct ShapTabDev {
 };
 
 template <int TPR, int ILP>
-__global__ void __launch_bounds__(TAB_ROWS * TPR, 1024 / (TAB_ROWS * TPR))
+__global__ void __launch_bounds__(TAB_ROWS * TPR, 2048 / (TAB_ROWS * TPR))
 k_shap_table(ShapTabDev P, const float* __restrict__ X, size_t n, int F, float missing, unsigned row_blocks,
              double* __restrict__ acc) {
   extern __shared__ float ph[];  // [chunk features][TAB_ROWS], then xs
