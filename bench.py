@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--only", choices=["c0", "c2", "c3", "serve", "prediction"], default=None,
+                    help="run one extra leg alone on GPU 0 and print its JSON (profiling aid)")
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-train-rows", type=int, default=1_000_000)
@@ -238,14 +240,10 @@ def _latency_summary(lat, rows, kinds, wall):
             "rows_per_s": float(rows.sum() / wall)}
 
 
-def serving_leg(sb, ctx, args, torch):
-    """The serving workload: a 1000-tree depth-8 ensemble trained on the
-    binary_mixed data (100 features), a Poisson request stream, rows per
-    request log-uniform in [1, 65536] (N(0,1) with 10% NaN), 90% margin and
-    10% TreeSHAP. Continuous batching (sb_server) against the same stream
-    served one request at a time by sb_predict_margin / sb_predict_contribs
-    ("plain GPU"). Latency = scheduled arrival to result on the host."""
-    import threading
+def serving_model(sb, ctx, args, torch):
+    """The serving workload's model: 1000 trees of depth 8 (binary:logistic)
+    trained on binary_mixed rows, and a pool of 65,536 request rows (N(0,1),
+    10% NaN, pinned host memory)."""
     from sequoia_boost_b200 import datagen
     n = args.serve_train_rows
     x, y = datagen.binary_mixed(n=n, seed=args.seed + 100)
@@ -256,11 +254,49 @@ def serving_leg(sb, ctx, args, torch):
     b.update(1000)
     model = b.model()
     del b, gh, x, y
-    F = 100
     rng = np.random.default_rng(args.seed + 200)
-    pool = rng.standard_normal((65536, F)).astype(np.float32)
+    pool = rng.standard_normal((65536, 100)).astype(np.float32)
     pool[rng.random(pool.shape) < 0.1] = np.nan
     pool = torch.from_numpy(pool).pin_memory().numpy()
+    return model, pool, rng
+
+
+def prediction_figures(sb, model, pool):
+    """Whole-call throughput of predict_contribs, predict_interactions and
+    predict_leaf on the serving model (host buffers, copies included), best
+    of 3 after one untimed call."""
+    out = {}
+    for name, rows, fn in (("contribs_rows_per_s", 4096, model.predict_contribs),
+                           ("interactions_rows_per_s", 128, model.predict_interactions),
+                           ("leaf_rows_per_s", 65536, model.predict_leaf)):
+        d = sb.DMatrix(pool[:rows])
+        fn(d)
+        best = math.inf
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fn(d)
+            best = min(best, time.perf_counter() - t0)
+        out[name] = rows / best
+    return out
+
+
+def prediction_leg(sb, ctx, args, torch):
+    model, pool, _ = serving_model(sb, ctx, args, torch)
+    return {"workload": f"1000-tree depth-8 binary:logistic ensemble (trained on {args.serve_train_rows} "
+                        "binary_mixed rows), 100 features", "prediction": prediction_figures(sb, model, pool)}
+
+
+def serving_leg(sb, ctx, args, torch):
+    """The serving workload: a 1000-tree depth-8 ensemble trained on the
+    binary_mixed data (100 features), a Poisson request stream, rows per
+    request log-uniform in [1, 65536] (N(0,1) with 10% NaN), 90% margin and
+    10% TreeSHAP. Continuous batching (sb_server) against the same stream
+    served one request at a time by sb_predict_margin / sb_predict_contribs
+    ("plain GPU"). Latency = scheduled arrival to result on the host."""
+    import threading
+    n = args.serve_train_rows
+    model, pool, rng = serving_model(sb, ctx, args, torch)
+    F = 100
     N = args.serve_requests
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, N))
     rows = np.clip(np.exp(rng.uniform(0.0, np.log(65536.0), N)).astype(np.int64), 1, 65536)
@@ -324,26 +360,9 @@ def serving_leg(sb, ctx, args, torch):
         wall = max(time.perf_counter() - t0, 1e-9)
         return _latency_summary(lat, rows, kinds, wall)
 
-    def run_prediction():
-        """Whole-call throughput of the other prediction entry points on the
-        same model (host buffers, copies included), best of 3."""
-        out = {}
-        for name, rows, fn in (("contribs_rows_per_s", 4096, model.predict_contribs),
-                               ("interactions_rows_per_s", 128, model.predict_interactions),
-                               ("leaf_rows_per_s", 65536, model.predict_leaf)):
-            d = sb.DMatrix(pool[:rows])
-            fn(d)
-            best = math.inf
-            for _ in range(3):
-                t0 = time.perf_counter()
-                fn(d)
-                best = min(best, time.perf_counter() - t0)
-            out[name] = rows / best
-        return out
-
     batched = run_batched()
     plain = run_plain()
-    pred = run_prediction()
+    pred = prediction_figures(sb, model, pool)
     return {"workload": f"1000-tree depth-8 binary:logistic ensemble (trained on {n} binary_mixed rows), "
                         f"{N} requests, Poisson {args.serve_rate:g} req/s, rows log-uniform [1, 65536], "
                         "10% NaN, 90% margin / 10% TreeSHAP",
@@ -473,6 +492,14 @@ def main():
     import torch
     import __graft_entry__ as ge
     torch.cuda.set_device(local)
+    if args.only:
+        sb = ge.load_package()
+        ctx = sb.Context(local)
+        leg = {"c0": lambda: c0_leg(sb, ctx, args), "c2": lambda: c2_leg(sb, ctx, args, torch),
+               "c3": lambda: c3_leg(sb, ctx, args), "serve": lambda: serving_leg(sb, ctx, args, torch),
+               "prediction": lambda: prediction_leg(sb, ctx, args, torch)}[args.only]
+        print(json.dumps({"leg": args.only, **leg()}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime

@@ -142,3 +142,53 @@ def test_xgboost_json_roundtrip_on_device(sb, ctx, tmp_path, objective):
         assert np.array_equal(a[1][key], b[1][key]), key
     d = sb.DMatrix(x)
     assert np.max(np.abs(m.predict(d) - r.predict(d))) < 1e-5
+
+
+def _chain_data(n, f, seed):
+    """y = the number of leading features (0, 1, 2, ...) above 0.1: every node
+    of the chain x_0 > 0.1, x_1 > 0.1, ... has its best split on the next
+    feature, so a lossguide tree grows one path through all f features."""
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, f), dtype=np.float32)
+    y = np.cumprod(x > 0.1, axis=1).sum(axis=1).astype(np.float32)
+    return x, y
+
+
+def _max_distinct_features(nodes, lo, hi):
+    """Most distinct split features on a root-to-leaf path of one tree."""
+    best = 0
+    stack = [(0, frozenset())]
+    while stack:
+        i, feats = stack.pop()
+        nd = nodes[lo + i]
+        if nd["left"] == -1:
+            best = max(best, len(feats))
+            continue
+        fs = feats | {int(nd["split_feature"])}
+        stack.append((int(nd["left"]), fs))
+        stack.append((int(nd["right"]), fs))
+    return best
+
+
+@pytest.mark.parametrize("f", [12, 30])
+def test_contribs_of_deep_lossguide_paths(sb, ctx, orc, f):
+    """shap.rs:321-367 on paths longer than the table form (10 features) and
+    the register form (12) hold: lossguide trees with max_depth 0 whose paths
+    split on 12 and on 30 distinct features. Contributions match the oracle's
+    recursion within 1e-4 and add up to the margins."""
+    x, y = _chain_data(40_000, f, seed=f)
+    p = sb.TrainingParams(objective="reg:squarederror", grow_policy="lossguide", max_leaves=64, max_depth=0,
+                          eta=0.5)
+    r = orc.train(x, y, p, 3)
+    arrays, base = r["model"].export(), r["model"].base_score
+    off, nodes = arrays[0], arrays[1]
+    deepest = max(_max_distinct_features(nodes, off[t], off[t + 1]) for t in range(len(off) - 1))
+    assert deepest >= min(f, 20), deepest
+    m = sb.BoostedModel.from_arrays(*arrays[:4], base, 0, f, objective=p.objective, ctx=ctx)
+    xt = x[:3000]
+    got = m.predict_contribs(sb.DMatrix(xt))
+    want = orc.predict_contribs(arrays, xt, base, 0)
+    assert np.max(np.abs(got - want)) < 1e-4
+    margin = orc.predict_margin(arrays, xt, base, 0)
+    sums = got.reshape(len(xt), f + 1).astype(np.float64).sum(axis=1)
+    assert np.max(np.abs(sums - margin)) < 1e-4
