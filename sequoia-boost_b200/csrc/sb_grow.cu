@@ -276,13 +276,33 @@ __device__ __forceinline__ void row_gradient(int objective, int K, float spw, co
   }
 }
 
+// Batched launches over many boosters (sb_train_many): the x-blocks of one
+// launch are every job's own grid laid end to end, block x belongs to job j
+// when xoff[j] <= x < xoff[j + 1], and the kernel body runs with that job's
+// state and its block index within its own grid. A job given no blocks has
+// xoff[j] == xoff[j + 1].
+struct JobGrid {
+  const BState* states;  // [njobs]
+  const unsigned* xoff;  // [njobs + 1]
+  int njobs;
+};
+
+__device__ __forceinline__ int job_of(const JobGrid& J, unsigned x) {
+  int lo = 0, hi = J.njobs;  // the last job whose first block is <= x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (J.xoff[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 // Gradients of every row (train.rs:297-302) and the round's row subset
 // (sample_rows, train.rs:465-475). The subset goes to the root list compacted:
 // each block owns a contiguous chunk of rows, reserves its places with one
 // atomic per counter, and writes its sampled rows (ascending) to the front of
 // rows0 and the others to the back, so the per-node lists hold sampled rows
 // only; the rows left out get their leaf values from k_route_rest.
-__global__ void __launch_bounds__(256) k_gradient(BState S) {
+__device__ __forceinline__ void k_gradient_body(const BState& S, unsigned bx, unsigned gdx) {
   const unsigned long long round = *S.round + S.round_base;
   const uint64_t rk = sb_round_key(S.seed, round);
   float mg[16], mh[16];
@@ -292,8 +312,8 @@ __global__ void __launch_bounds__(256) k_gradient(BState S) {
   __shared__ unsigned int s_base[2], s_wk[8], s_wu[8];
   __shared__ unsigned int s_max[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const size_t per = (n + gridDim.x - 1) / gridDim.x;
-  const size_t lo = min(n, (size_t)blockIdx.x * per), hi = min(n, lo + per);
+  const size_t per = (n + gdx - 1) / gdx;
+  const size_t lo = min(n, (size_t)bx * per), hi = min(n, lo + per);
   // the caller's subset (flags in rows1), or the Bernoulli draw
   auto keep_of = [&](size_t r) -> bool {
     if (S.ext_gpair) return !(S.rows1[r] & UNSAMPLED);
@@ -379,16 +399,21 @@ __global__ void __launch_bounds__(256) k_gradient(BState S) {
   __syncthreads();
   if (S.fixed && tid < 2 * K && tid < 32 && s_max[tid]) atomicMax(&S.maxabs[tid], s_max[tid]);
 }
+__global__ void __launch_bounds__(256) k_gradient(BState S) { k_gradient_body(S, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_gradient_jobs(JobGrid J) {
+  const int j = job_of(J, blockIdx.x);
+  k_gradient_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j]);
+}
 
 // Leaf values of the rows outside the round's subset (rows0[n - unkept, n)):
 // each is routed through the round's K trees in bin space, as the partition
 // routes sampled rows (missing -> default_left; categorical: the category
 // set; numeric: local bin <= split bin).
-__global__ void k_route_rest(BState S) {
+__device__ __forceinline__ void k_route_rest_body(const BState& S, unsigned bx, unsigned gdx) {
   const size_t n = S.n;
   const size_t un = *S.unkept;
   const unsigned long long round = *S.round;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < un; i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t i = (size_t)bx * blockDim.x + threadIdx.x; i < un; i += (size_t)gdx * blockDim.x) {
     const uint32_t r = S.rows0[n - 1 - i];
     for (int k = 0; k < S.K; ++k) {
       const sb_node* out = S.out_nodes + ((size_t)round * S.K + k) * S.maxn;
@@ -406,6 +431,11 @@ __global__ void k_route_rest(BState S) {
     }
     if (S.row_leaf) S.row_leaf[r] = -1;
   }
+}
+__global__ void k_route_rest(BState S) { k_route_rest_body(S, blockIdx.x, gridDim.x); }
+__global__ void k_route_rest_jobs(JobGrid J) {
+  const int j = job_of(J, blockIdx.x);
+  k_route_rest_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j]);
 }
 
 // Objective::gradient over caller-supplied margins (row-major [n][K]),
@@ -451,13 +481,13 @@ __device__ void node_feature_mask(const BState& S, int k, int nid, uint64_t tkey
 // Per round, one CTA per class tree: quantisation scales, the sampled-row
 // fallback, the tree's colsample_bytree pool (train.rs:479-489) and its root.
 constexpr int PREP_THREADS = 128;
-__global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
+__device__ __forceinline__ void k_round_prep_body(const BState& S, unsigned bx, unsigned gdx) {
   __shared__ uint32_t s_a[4096];
   __shared__ uint32_t s_b[4096];
   __shared__ uint32_t s_mask[128];
   __shared__ int s_len;
   const unsigned long long round = *S.round + S.round_base;
-  const int k = blockIdx.x, tid = threadIdx.x;
+  const int k = bx, tid = threadIdx.x;
   const int F = S.F;
   const uint64_t tkey = sb_tree_key(S.seed, round, (uint64_t)(k + S.k_base));
   // the subset's size; an empty draw takes one row (train.rs:472-474)
@@ -568,13 +598,18 @@ __global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) {
     node_feature_mask(S, k, 0, tkey, S.fmask + NI(S, k, 0) * S.FW, nullptr, true,
                       S.samp_scratch ? S.samp_scratch + (size_t)k * S.F : nullptr);
 }
+__global__ void __launch_bounds__(PREP_THREADS) k_round_prep(BState S) { k_round_prep_body(S, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(PREP_THREADS) k_round_prep_jobs(JobGrid J) {
+  const int j = job_of(J, blockIdx.x);
+  k_round_prep_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j]);
+}
 
 // FIXED: q = rint(x * 2^s), packed (q_g << 32) + q_h.
-__global__ void k_quantize(BState S) {
+__device__ __forceinline__ void k_quantize_body(const BState& S, unsigned bx, unsigned gdx) {
   float eg = 0.0f, eh = 0.0f;
   const size_t total = (size_t)S.K * S.n;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t i = (size_t)bx * blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gdx * blockDim.x) {
     int k = (int)(i / S.n);
     float2 v = S.gpair[i];
     int sg = S.shifts[2 * k], sh = S.shifts[2 * k + 1];
@@ -597,6 +632,11 @@ __global__ void k_quantize(BState S) {
   }
   __syncthreads();
   if (threadIdx.x < 2 && s_e[threadIdx.x]) atomicMax((unsigned int*)&S.qerr[0] + threadIdx.x, s_e[threadIdx.x]);
+}
+__global__ void k_quantize(BState S) { k_quantize_body(S, blockIdx.x, gridDim.x); }
+__global__ void k_quantize_jobs(JobGrid J) {
+  const int j = job_of(J, blockIdx.x);
+  k_quantize_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j]);
 }
 
 // ---------------------------------------------------------------- K6
@@ -954,10 +994,10 @@ __device__ __forceinline__ bool in_mask(const uint32_t* m, int f) { return (m[f 
 // feature's bins of a node whose histogram is the parent's minus the built
 // sibling's (the subtraction trick, K5), then record the feature's best
 // candidate gain (-inf when the node may not use the feature).
-__global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) {
+__device__ __forceinline__ void k_eval_scan_body(const BState& S, unsigned bx, unsigned gdx, int d) {
   extern __shared__ double ev_sm[];
-  const int slot = blockIdx.x, k = blockIdx.z;
-  if (slot >= S.lvl_count[k]) return;
+  const int slot = bx, k = blockIdx.z;
+  if (k >= S.K || slot >= S.lvl_count[k]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pi = blockIdx.y * SCAN_WARPS + warp;
   if (pi >= S.upool_len[k]) return;
@@ -991,15 +1031,20 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) {
   }
   if (lane == 0) S.mbuf[((size_t)k * S.maxw + slot) * S.F + f] = m;
 }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan(BState S, int d) { k_eval_scan_body(S, blockIdx.x, gridDim.x, d); }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_scan_jobs(JobGrid J, int d) {
+  const int j = job_of(J, blockIdx.x);
+  k_eval_scan_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d);
+}
 
 // Phase 2a, one warp per (frontier node, usable pool feature): with Q = the
 // best gain of the node's earlier features (or 0), find this feature's last
 // certain record and its ambiguous records (FeatRec).
-__global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) {
+__device__ __forceinline__ void k_eval_records_body(const BState& S, unsigned bx, unsigned gdx, int d) {
   extern __shared__ double ev_sm[];
   __shared__ double s_gains[SCAN_WARPS][64];
-  const int slot = blockIdx.x, k = blockIdx.z;
-  if (slot >= S.lvl_count[k]) return;
+  const int slot = bx, k = blockIdx.z;
+  if (k >= S.K || slot >= S.lvl_count[k]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pi = blockIdx.y * SCAN_WARPS + warp;
   if (pi >= S.upool_len[k]) return;
@@ -1027,16 +1072,22 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) 
   CatScratch* cs = S.cat_cap > 0 ? &csv : nullptr;
   scan_feature<SCAN_RECORDS>(S, frontier_hist(S, d, k, slot), k, f, E, q, cs, s_gains[warp], nullptr, rec);
 }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_records(BState S, int d) { k_eval_records_body(S, blockIdx.x, gridDim.x, d); }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_records_jobs(JobGrid J, int d) {
+  const int j = job_of(J, blockIdx.x);
+  k_eval_records_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d);
+}
 
 // Phase 2b, one warp per frontier node: the winner of consider's sequential
 // rule is the last certain record over all features, followed by a short
 // sequential resolution over the ambiguous records after it.
-__global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
+__device__ __forceinline__ void k_eval_pick_body(const BState& S, unsigned bx, unsigned gdx, int d) {
   extern __shared__ double ev_sm[];
   __shared__ NodeSplit s_best[SCAN_WARPS];
   __shared__ double s_gains[SCAN_WARPS][64];
   const int k = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int slot = blockIdx.x * SCAN_WARPS + warp;
+  if (k >= S.K) return;
+  const int slot = bx * SCAN_WARPS + warp;
   if (slot >= S.lvl_count[k]) return;
   const int nid = S.lvl_begin[k] + slot;
   const size_t ni = NI(S, k, nid);
@@ -1124,6 +1175,11 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) {
     for (int i = lane; i < best->ncat; i += 32) o.cat_order[i] = best->cat_order[i];
   }
 }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick(BState S, int d) { k_eval_pick_body(S, blockIdx.x, gridDim.x, d); }
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_pick_jobs(JobGrid J, int d) {
+  const int j = job_of(J, blockIdx.x);
+  k_eval_pick_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d);
+}
 
 __device__ sb_node make_leaf(float value, float sum_hess) {  // Node::leaf, regtree.rs:51-65
   sb_node nd;
@@ -1145,7 +1201,7 @@ __device__ sb_node make_leaf(float value, float sum_hess) {  // Node::leaf, regt
 // Expand the frontier of level d: child ids in the reference's order
 // (left = num_nodes + 2 * rank among split nodes), child state, final leaf
 // values, and the level's partition tiles.
-__global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tiles) {
+__device__ __forceinline__ void k_assign_body(const BState& S, unsigned bx, unsigned gdx, int d, int write_tiles) {
   __shared__ int sm_i[33];
   __shared__ int s_tile_carry;
   __shared__ int s_toff[1024], s_nid[1024];
@@ -1153,7 +1209,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
   const unsigned long long round = *S.round;
   const int tid = threadIdx.x;
   const bool last = !S.lossguide && (d + 1 == S.max_depth);
-  for (int k = blockIdx.x; k < S.K; k += gridDim.x) {  // one class tree per block
+  for (int k = bx; k < S.K; k += gdx) {  // one class tree per block
     const int begin = S.lvl_begin[k], cnt = S.lvl_count[k], nn0 = S.num_nodes[k];
     if (write_tiles) {  // reserve the tree's partition tiles (their order in the list is free)
       int mine = 0;
@@ -1244,7 +1300,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
           S.split[ri].valid = 0;
           // the launch has at most 1024 threads in all when per-node sampling is on
           uint32_t* scratch =
-              S.samp_scratch ? S.samp_scratch + ((size_t)blockIdx.x * blockDim.x + tid) * S.F : nullptr;
+              S.samp_scratch ? S.samp_scratch + ((size_t)bx * blockDim.x + tid) * S.F : nullptr;
           if (!last) {
             node_feature_mask(S, k, left, tkey, S.fmask + li * S.FW, S.allowed + li * S.FW, call, scratch);
             node_feature_mask(S, k, right, tkey, S.fmask + ri * S.FW, S.allowed + ri * S.FW, call, scratch);
@@ -1305,6 +1361,11 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
     __syncthreads();
   }
 }
+__global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tiles) { k_assign_body(S, blockIdx.x, gridDim.x, d, write_tiles); }
+__global__ void __launch_bounds__(1024) k_assign_jobs(JobGrid J, int d, int write_tiles) {
+  const int j = job_of(J, blockIdx.x);
+  k_assign_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d, write_tiles);
+}
 
 // K7 + K8: partition every split node's rows into its two children (left rows
 // fill the segment from its start, right rows from its end), and the margin
@@ -1316,7 +1377,7 @@ __global__ void __launch_bounds__(1024) k_assign(BState S, int d, int write_tile
 constexpr int PART_THREADS = 256;
 constexpr int PART_WARPS = PART_THREADS / 32;
 constexpr int PART_STEPS = PART_TILE / PART_THREADS;  // 32-row steps per warp
-__global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) {
+__device__ __forceinline__ void k_partition_body(const BState& S, unsigned bx, unsigned gdx, int d) {
   __shared__ unsigned int s_wl[PART_WARPS], s_wa[PART_WARPS];
   __shared__ unsigned int s_base[2];
   const bool last = !S.lossguide && (d + 1 == S.max_depth);
@@ -1327,7 +1388,7 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
   const int K = S.K;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (int t = bx; t < ntiles; t += gdx) {
     const int4 tile = S.ptiles[t];
     const int k = tile.x, nid = tile.y;
     const size_t ni = NI(S, k, nid);
@@ -1430,11 +1491,16 @@ __global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) 
     __syncthreads();
   }
 }
+__global__ void __launch_bounds__(PART_THREADS, 4) k_partition(BState S, int d) { k_partition_body(S, blockIdx.x, gridDim.x, d); }
+__global__ void __launch_bounds__(PART_THREADS, 4) k_partition_jobs(JobGrid J, int d) {
+  const int j = job_of(J, blockIdx.x);
+  k_partition_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d);
+}
 
 // After the partition: children segments and sampled counts, the smaller
 // child to build (hist.rs:352-362: left when left_rows <= right_rows), and
 // the histogram work list of level d + 1.
-__global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
+__device__ __forceinline__ void k_plan_body(const BState& S, unsigned bx, unsigned gdx, int d) {
   constexpr int GROUP = 1024;  // class trees per pass over the (tree, node) pairs
   __shared__ int sm_i[33];
   __shared__ unsigned long long sm_u[33];
@@ -1525,6 +1591,11 @@ __global__ void __launch_bounds__(1024) k_plan(BState S, int d) {
     S.prefix[s_items] = s_pos;
     *S.ptile_count = 0;  // the partition has consumed this level's tiles
   }
+}
+__global__ void __launch_bounds__(1024) k_plan(BState S, int d) { k_plan_body(S, blockIdx.x, gridDim.x, d); }
+__global__ void __launch_bounds__(1024) k_plan_jobs(JobGrid J, int d) {
+  const int j = job_of(J, blockIdx.x);
+  k_plan_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j], d);
 }
 
 // ------------------------------------------------------- lossguide growth
@@ -1704,7 +1775,7 @@ __global__ void k_apply_delta(float* __restrict__ margin, const float* __restric
     margin[i] = __fadd_rn(margin[i], delta[i]);
 }
 
-__global__ void k_round_end(BState S) {
+__device__ __forceinline__ void k_round_end_body(const BState& S, unsigned bx, unsigned gdx) {
   const unsigned long long round = *S.round;
   for (int k = threadIdx.x; k < S.K; k += blockDim.x) {
     size_t t = (size_t)round * S.K + k;
@@ -1719,6 +1790,11 @@ __global__ void k_round_end(BState S) {
     if (S.fixed)
       for (int i = 0; i < 2 * S.K; ++i) S.maxabs[i] = 0u;
   }
+}
+__global__ void k_round_end(BState S) { k_round_end_body(S, blockIdx.x, gridDim.x); }
+__global__ void k_round_end_jobs(JobGrid J) {
+  const int j = job_of(J, blockIdx.x);
+  k_round_end_body(J.states[j], blockIdx.x - J.xoff[j], J.xoff[j + 1] - J.xoff[j]);
 }
 
 }  // namespace
@@ -2515,6 +2591,244 @@ int booster_run(sb_booster* b, int n_rounds) {
   for (int r = 0; r < n_rounds; ++r) {
     SB_TRY(booster_round(b));
     b->rounds_done++;
+  }
+  return SB_OK;
+}
+
+// ------------------------------------------------------------ batched jobs
+// Depthwise boosters of one device trained together (sb_train_many): every
+// round is one launch per kernel step over all jobs, whose grids are laid end
+// to end (JobGrid), recorded once as a CUDA graph and replayed. A job runs
+// the same kernel bodies on its own state as when it trains alone, so its
+// model is the same; a job deeper than others simply gets no blocks in the
+// launches of the levels it does not have.
+bool booster_batchable(const sb_booster* b) {
+  return b && !b->lossguide && !b->ext && !b->timing && b->evals.empty() && b->S.row_leaf == nullptr &&
+         b->g->layout == HIST_LAYOUT_TILED;
+}
+
+int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int rounds) {
+  if (nb <= 0 || rounds <= 0) return SB_OK;
+  const int fixed = bs[0]->S.fixed;
+  int maxD = 0, maxK = 1;
+  size_t esm = 0;
+  for (int j = 0; j < nb; ++j) {
+    sb_booster* b = bs[j];
+    SB_REQUIRE(booster_batchable(b) && b->S.fixed == fixed, SB_ERR_INVALID_ARG, "internal: job %d not batchable", j);
+    SB_CUDA(cudaStreamSynchronize(b->ctx->stream));  // its set-up work
+    SB_TRY(booster_alloc_trees(b, (b->rounds_done + rounds) * b->K));
+    SB_TRY(booster_set_eval_smem(b));
+    SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    maxD = std::max(maxD, b->D);
+    maxK = std::max(maxK, b->K);
+    esm = std::max(esm, eval_smem(b));
+  }
+  SB_TRY(raise_smem_limit((const void*)k_eval_scan_jobs, esm));
+  SB_TRY(raise_smem_limit((const void*)k_eval_records_jobs, esm));
+  SB_TRY(raise_smem_limit((const void*)k_eval_pick_jobs, esm));
+  // the histogram launches' per-job descriptions
+  std::vector<HistLaunch> Ls(nb);
+  for (int j = 0; j < nb; ++j) {
+    const sb_booster* b = bs[j];
+    const BState& S = b->S;
+    HistLaunch& L = Ls[j];
+    L.g = b->g;
+    L.gpair = S.fixed ? (const void*)S.gpk : (const void*)S.gpair;
+    L.fixed = S.fixed;
+    L.quant_bits = S.bits;
+    L.items = S.items;
+    L.prefix = S.prefix;
+    L.count = S.item_count;
+    L.max_items = 0;
+    L.tiles = b->d_tiles.p;
+    L.ntiles = (int)b->g->tiles.size();
+    L.rows_done = nullptr;
+    L.pool_mask = S.pool_mask;
+    L.rows_bound = b->n * (size_t)b->K;
+  }
+  HistJobsPlan hp;
+  SB_TRY(hist_jobs_prepare(ctx, Ls, &hp));
+  // block offsets of every launch step, in one device table
+  struct Step {
+    size_t off = 0;
+    unsigned blocks = 0;
+  };
+  std::vector<unsigned> tab;
+  auto step = [&](auto blocks_of) {
+    Step st;
+    st.off = tab.size();
+    tab.push_back(0);
+    for (int j = 0; j < nb; ++j) {
+      st.blocks += (unsigned)blocks_of(j);
+      tab.push_back(st.blocks);
+    }
+    return st;
+  };
+  auto gblocks = [&](int j) { return std::min<size_t>((bs[j]->n + 255) / 256, (size_t)ctx->num_sms * 16); };
+  const Step s_grad = step(gblocks);
+  const Step s_prep = step([&](int j) { return bs[j]->K; });
+  const Step s_quant = step([&](int j) { return fixed ? gblocks(j) : 0; });
+  const Step s_hist0 = step([&](int j) { return hp.hist_grid[j]; });
+  const Step s_zero0 = step([&](int j) { return hp.zero_grid[j]; });
+  std::vector<Step> s_scan(maxD), s_pick(maxD), s_assign(maxD), s_part(maxD), s_plan(maxD), s_hist(maxD),
+      s_zero(maxD);
+  std::vector<unsigned> fy(maxD, 1);
+  std::vector<int> items(maxD, 0);
+  for (int d = 0; d < maxD; ++d) {
+    auto width = [&](int j) { return (unsigned)std::min(1 << d, bs[j]->maxw); };
+    auto act = [&](int j) { return d < bs[j]->D; };
+    auto build = [&](int j) { return d + 1 < bs[j]->D; };
+    s_scan[d] = step([&](int j) { return act(j) ? width(j) : 0u; });
+    s_pick[d] = step([&](int j) { return act(j) ? (width(j) + SCAN_WARPS - 1) / SCAN_WARPS : 0u; });
+    s_assign[d] = step([&](int j) { return act(j) ? assign_blocks(bs[j], 1024) : 0u; });
+    s_part[d] = step([&](int j) {
+      return act(j) ? part_blocks(ctx, bs[j]->n, bs[j]->K, (size_t)bs[j]->K * width(j)) : 0u;
+    });
+    s_plan[d] = step([&](int j) { return build(j) ? 1u : 0u; });
+    s_hist[d] = step([&](int j) { return build(j) ? hp.hist_grid[j] : 0u; });
+    s_zero[d] = step([&](int j) { return build(j) ? hp.zero_grid[j] : 0u; });
+    for (int j = 0; j < nb; ++j) {
+      if (act(j)) fy[d] = std::max(fy[d], (unsigned)((bs[j]->g->F + SCAN_WARPS - 1) / SCAN_WARPS));
+      if (build(j)) items[d] = std::max(items[d], bs[j]->K * (1 << d));
+    }
+  }
+  const Step s_route = step(gblocks);
+  const Step s_end = step([&](int) { return 1; });
+  DBuf<unsigned> d_tab;
+  DBuf<BState> d_states, d_states_g;
+  SB_TRY(d_tab.alloc(ctx, tab.size()));
+  SB_TRY(d_states.alloc(ctx, nb));
+  SB_TRY(d_states_g.alloc(ctx, nb));
+  SB_CUDA(cudaMemcpyAsync(d_tab.p, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  auto J = [&](const BState* states, const Step& st) { return JobGrid{states, d_tab.p + st.off, nb}; };
+  auto body = [&]() -> int {
+    SB_LAUNCH(ctx, k_gradient_jobs, s_grad.blocks, 256, 0, J(d_states_g.p, s_grad));
+    SB_LAUNCH(ctx, k_round_prep_jobs, s_prep.blocks, PREP_THREADS, 0, J(d_states.p, s_prep));
+    if (fixed) SB_LAUNCH(ctx, k_quantize_jobs, s_quant.blocks, 256, 0, J(d_states.p, s_quant));
+    SB_TRY(launch_hist_jobs(ctx, hp, d_tab.p + s_hist0.off, s_hist0.blocks, d_tab.p + s_zero0.off, s_zero0.blocks,
+                            maxK));
+    for (int d = 0; d < maxD; ++d) {
+      if (s_scan[d].blocks == 0) break;
+      const dim3 sg(s_scan[d].blocks, fy[d], (unsigned)maxK);
+      SB_LAUNCH(ctx, k_eval_scan_jobs, sg, EVAL_THREADS, esm, J(d_states.p, s_scan[d]), d);
+      SB_LAUNCH(ctx, k_eval_records_jobs, sg, EVAL_THREADS, esm, J(d_states.p, s_scan[d]), d);
+      SB_LAUNCH(ctx, k_eval_pick_jobs, dim3(s_pick[d].blocks, (unsigned)maxK), EVAL_THREADS, esm,
+                J(d_states.p, s_pick[d]), d);
+      SB_LAUNCH(ctx, k_assign_jobs, s_assign[d].blocks, 1024, 0, J(d_states.p, s_assign[d]), d, 1);
+      SB_LAUNCH(ctx, k_partition_jobs, s_part[d].blocks, PART_THREADS, 0, J(d_states.p, s_part[d]), d);
+      if (s_plan[d].blocks) {
+        SB_LAUNCH(ctx, k_plan_jobs, s_plan[d].blocks, 1024, 0, J(d_states.p, s_plan[d]), d);
+        SB_TRY(launch_hist_jobs(ctx, hp, d_tab.p + s_hist[d].off, s_hist[d].blocks, d_tab.p + s_zero[d].off,
+                                s_zero[d].blocks, items[d]));
+      }
+    }
+    SB_LAUNCH(ctx, k_route_rest_jobs, s_route.blocks, 256, 0, J(d_states.p, s_route));
+    SB_LAUNCH(ctx, k_round_end_jobs, s_end.blocks, 32, 0, J(d_states.p, s_end));
+    return SB_OK;
+  };
+  // the jobs' states: the gradient pass folds in the last tree's leaf values
+  // from the second round of a fresh booster on
+  std::vector<BState> hs(nb), hg(nb), ug(nb);
+  for (int j = 0; j < nb; ++j) {
+    std::memcpy(&hs[j], &bs[j]->S, sizeof(BState));
+    hs[j].apply_delta = 0;
+  }
+  SB_CUDA(cudaMemcpyAsync(d_states.p, hs.data(), nb * sizeof(BState), cudaMemcpyHostToDevice, ctx->stream));
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_nodes = 0;
+  int rc = SB_OK;
+  bool uploaded = false;
+  for (int r = 0; r < rounds && rc == SB_OK; ++r) {
+    for (int j = 0; j < nb; ++j) {
+      std::memcpy(&hg[j], &hs[j], sizeof(BState));
+      hg[j].apply_delta = bs[j]->delta_pending ? 1 : 0;
+    }
+    if (!uploaded || std::memcmp(hg.data(), ug.data(), nb * sizeof(BState)) != 0) {
+      const cudaError_t e = cudaMemcpyAsync(d_states_g.p, hg.data(), nb * sizeof(BState), cudaMemcpyHostToDevice,
+                                            ctx->stream);
+      if (e != cudaSuccess) {
+        rc = cuda_status(e, "cudaMemcpyAsync", __FILE__, __LINE__);
+        break;
+      }
+      std::memcpy(ug.data(), hg.data(), nb * sizeof(BState));
+      uploaded = true;
+    }
+    if (!exec) {  // record the round once; it reads the jobs' states from device memory
+      const uint64_t l0 = ctx->launches;
+      cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        rc = cuda_status(e, "cudaStreamBeginCapture", __FILE__, __LINE__);
+        break;
+      }
+      rc = body();
+      cudaGraph_t graph = nullptr;
+      e = cudaStreamEndCapture(ctx->stream, &graph);
+      graph_nodes = ctx->launches - l0;
+      ctx->launches = l0;  // recorded, not launched
+      if (rc == SB_OK && e != cudaSuccess) rc = cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+      if (rc == SB_OK) {
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) rc = cuda_status(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+      }
+      if (graph) cudaGraphDestroy(graph);
+      if (rc != SB_OK) break;
+    }
+    const cudaError_t e = cudaGraphLaunch(exec, ctx->stream);
+    if (e != cudaSuccess) {
+      rc = cuda_status(e, "cudaGraphLaunch", __FILE__, __LINE__);
+      break;
+    }
+    ctx->launches += graph_nodes;
+    for (int j = 0; j < nb; ++j) {
+      bs[j]->rounds_done++;
+      bs[j]->delta_pending = bs[j]->S.update_margin != 0;
+    }
+  }
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (rc == SB_OK && se != cudaSuccess) rc = cuda_status(se, "cudaStreamSynchronize", __FILE__, __LINE__);
+  for (int j = 0; j < nb; ++j) bs[j]->stats.rounds = bs[j]->rounds_done;
+  return rc;
+}
+
+int boosters_train_many(sb_ctx* ctx, sb_booster* const* bs, const int* rounds, int nb, int* status) {
+  // the batchable boosters of the more common precision train together
+  int nfix = 0, nflt = 0;
+  for (int j = 0; j < nb; ++j)
+    if (status[j] == SB_OK && bs[j] && rounds[j] > 0 && booster_batchable(bs[j])) (bs[j]->S.fixed ? nfix : nflt)++;
+  const int bfixed = nfix >= nflt ? 1 : 0;
+  std::vector<int> batch, rest;
+  for (int j = 0; j < nb; ++j) {
+    if (status[j] != SB_OK || !bs[j] || rounds[j] <= 0) continue;
+    if (booster_batchable(bs[j]) && bs[j]->S.fixed == bfixed && nfix + nflt > 1) batch.push_back(j);
+    else rest.push_back(j);
+  }
+  // the others: round r of each before round r + 1 of any, on their own streams
+  int max_rest = 0;
+  for (int j : rest) max_rest = std::max(max_rest, rounds[j]);
+  for (int r = 0; r < max_rest; ++r)
+    for (int j : rest)
+      if (status[j] == SB_OK && r < rounds[j]) {
+        status[j] = booster_run(bs[j], 1);
+        bs[j]->stats.rounds = bs[j]->rounds_done;
+      }
+  // the batch, in segments of rounds that all its remaining jobs still have
+  int done = 0;
+  while (!batch.empty()) {
+    int seg = INT32_MAX;
+    for (int j : batch) seg = std::min(seg, rounds[j] - done);
+    std::vector<sb_booster*> part;
+    for (int j : batch) part.push_back(bs[j]);
+    const int rc = boosters_train_batched(ctx, part.data(), (int)part.size(), seg);
+    if (rc != SB_OK) {
+      for (int j : batch) status[j] = rc;
+      return rc;
+    }
+    done += seg;
+    std::vector<int> next;
+    for (int j : batch)
+      if (rounds[j] > done) next.push_back(j);
+    batch.swap(next);
   }
   return SB_OK;
 }

@@ -88,7 +88,7 @@ __device__ __forceinline__ void add_pair(unsigned a, unsigned hoff, uint32_t vg,
 // int32 / uint32 integers; FP32: floats), so a warp's atomics spread over all
 // 32 banks. Every entry costs one add into each plane.
 template <bool FIXED>
-__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
+__device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, unsigned gdx) {
   extern __shared__ unsigned long long sh_u64[];
   unsigned* sh_g = reinterpret_cast<unsigned*>(sh_u64);
   __shared__ double s_tot_d[2];
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
   const uint64_t W = a.prefix[count];
   if (W == 0) return;
   const uint64_t U = W * (uint64_t)a.ntiles;
-  const uint64_t lo = U * blockIdx.x / gridDim.x, hi = U * (blockIdx.x + 1) / gridDim.x;
+  const uint64_t lo = U * bx / gdx, hi = U * (bx + 1) / gdx;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
   uint64_t u = lo;
@@ -269,6 +269,35 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
     __syncthreads();
     u += n_pos;
   }
+}
+
+template <bool FIXED>
+__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
+  hist_tiled_body<FIXED>(a, blockIdx.x, gridDim.x);
+}
+
+// Many indexes' histogram launches as one (sb_train_many): the x-blocks are
+// every job's own persistent grid laid end to end; block x belongs to job j
+// when xoff[j] <= x < xoff[j + 1], and runs job j's launch description.
+struct HistJobs {
+  const HistDev* devs;   // [njobs]
+  const unsigned* xoff;  // [njobs + 1]
+  int njobs;
+};
+
+__device__ __forceinline__ int hist_job_of(const unsigned* xoff, int njobs, unsigned x) {
+  int lo = 0, hi = njobs;  // the last job whose first block is <= x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (xoff[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <bool FIXED>
+__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_jobs(HistJobs H) {
+  const int j = hist_job_of(H.xoff, H.njobs, blockIdx.x);
+  hist_tiled_body<FIXED>(H.devs[j], blockIdx.x - H.xoff[j], H.xoff[j + 1] - H.xoff[j]);
 }
 
 // LANES layout (see sb_internal.cuh): lane l of every warp owns the features
@@ -459,6 +488,19 @@ __global__ void k_zero_items(const HistItem* __restrict__ items, const int* __re
     o[i] = 0ull;
   if (items[it].root && blockIdx.x == 0 && threadIdx.x < 2)
     reinterpret_cast<unsigned long long*>(items[it].total)[threadIdx.x] = 0ull;
+}
+
+// k_zero_items for many jobs: job j's blocks are xoff[j] .. xoff[j + 1] - 1.
+__global__ void k_zero_items_jobs(const ZeroJob* __restrict__ zj, const unsigned* __restrict__ xoff, int njobs) {
+  const int j = hist_job_of(xoff, njobs, blockIdx.x);
+  const unsigned bx = blockIdx.x - xoff[j], gdx = xoff[j + 1] - xoff[j];
+  const ZeroJob z = zj[j];
+  const int it = blockIdx.y;
+  if (it >= *z.count) return;
+  unsigned long long* o = reinterpret_cast<unsigned long long*>(z.items[it].out);
+  for (size_t i = (size_t)bx * blockDim.x + threadIdx.x; i < z.words; i += (size_t)gdx * blockDim.x) o[i] = 0ull;
+  if (z.items[it].root && bx == 0 && threadIdx.x < 2)
+    reinterpret_cast<unsigned long long*>(z.items[it].total)[threadIdx.x] = 0ull;
 }
 
 __global__ void k_subtract(const double2* __restrict__ p, const double2* __restrict__ c,
@@ -736,7 +778,8 @@ int hist_grid(sb_ctx* ctx, const Ghist* g, size_t rows_bound) {
   return (int)std::max<size_t>(1, std::min(full, want));
 }
 
-int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
+// The kernel's description of one launch.
+static HistDev hist_dev(const HistLaunch& L) {
   HistDev a;
   a.bins = L.g->bins.p;
   a.foff = L.g->foff.p;
@@ -755,6 +798,11 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   a.rows_done = L.rows_done;
   a.pool_mask = L.pool_mask;
   a.FW = (int)((L.g->F + 31) / 32);
+  return a;
+}
+
+int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
+  const HistDev a = hist_dev(L);
   const int grid = hist_grid(ctx, L.g, L.rows_bound);
   const size_t sm = L.g->hist_smem_bytes;
   void (*kern)(HistDev) = L.fixed ? k_hist<true> : k_hist<false>;
@@ -775,6 +823,51 @@ int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const 
   size_t words = (g->total_bins + g->F) * 2;
   dim3 grid((unsigned)std::min<size_t>((words + 255) / 256, 64), (unsigned)max_items);
   SB_LAUNCH(ctx, k_zero_items, grid, 256, 0, items, count, words);
+  return SB_OK;
+}
+
+int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPlan* P) {
+  const int nj = (int)Ls.size();
+  SB_REQUIRE(nj > 0, SB_ERR_INVALID_ARG, "internal: no jobs");
+  std::vector<HistDev> devs(nj);
+  std::vector<ZeroJob> zero(nj);
+  P->fixed = Ls[0].fixed;
+  P->smem = 0;
+  P->hist_grid.assign(nj, 0);
+  P->zero_grid.assign(nj, 0);
+  for (int j = 0; j < nj; ++j) {
+    const HistLaunch& L = Ls[j];
+    SB_REQUIRE(L.g->layout == HIST_LAYOUT_TILED && L.fixed == P->fixed, SB_ERR_INVALID_ARG,
+               "internal: batched histograms need the TILED layout and one precision");
+    devs[j] = hist_dev(L);
+    const size_t words = (L.g->total_bins + L.g->F) * 2;
+    zero[j] = ZeroJob{L.items, L.count, words};
+    P->hist_grid[j] = (unsigned)hist_grid(ctx, L.g, L.rows_bound);
+    P->zero_grid[j] = (unsigned)std::min<size_t>((words + 255) / 256, 64);
+    P->smem = std::max(P->smem, L.g->hist_smem_bytes);
+  }
+  P->njobs = nj;
+  cudaStream_t st = ctx->stream;
+  SB_TRY(P->devs.alloc(ctx, nj * sizeof(HistDev)));
+  SB_TRY(P->zero.alloc(ctx, nj));
+  SB_CUDA(cudaMemcpyAsync(P->devs.p, devs.data(), nj * sizeof(HistDev), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(P->zero.p, zero.data(), nj * sizeof(ZeroJob), cudaMemcpyHostToDevice, st));
+  SB_TRY(raise_smem_limit((const void*)k_hist_jobs<true>, P->smem));
+  SB_TRY(raise_smem_limit((const void*)k_hist_jobs<false>, P->smem));
+  SB_CUDA(cudaStreamSynchronize(st));  // the host tables are released on return
+  return SB_OK;
+}
+
+int launch_hist_jobs(sb_ctx* ctx, const HistJobsPlan& P, const unsigned* d_xoff, unsigned hist_blocks,
+                     const unsigned* d_zoff, unsigned zero_blocks, int max_items) {
+  if (max_items <= 0 || hist_blocks == 0) return SB_OK;
+  SB_LAUNCH(ctx, k_zero_items_jobs, dim3(zero_blocks, (unsigned)max_items), 256, 0, P.zero.p, d_zoff, P.njobs);
+  HistJobs H;
+  H.devs = reinterpret_cast<const HistDev*>(P.devs.p);
+  H.xoff = d_xoff;
+  H.njobs = P.njobs;
+  if (P.fixed) SB_LAUNCH(ctx, k_hist_jobs<true>, hist_blocks, HIST_THREADS, P.smem, H);
+  else SB_LAUNCH(ctx, k_hist_jobs<false>, hist_blocks, HIST_THREADS, P.smem, H);
   return SB_OK;
 }
 

@@ -195,7 +195,7 @@ int approx_cuts(ApproxState* A, const float* d_hess, Ghist* g);
 // ------------------------------------------------------------ histograms
 // One node histogram to accumulate: rows[begin..end) of a row list.
 struct HistItem {
-  const uint32_t* rows;  // row list (UNSAMPLED-flagged ids)
+  const uint32_t* rows;  // row list (the round's sampled rows)
   uint32_t begin, end;
   uint32_t k;            // class (gradient column)
   uint32_t root;         // 1: also accumulate the node total
@@ -219,6 +219,32 @@ struct HistLaunch {
   size_t rows_bound = 0;          // most rows one launch accumulates (0: unknown, full grid)
 };
 
+// Zeroing of one job's node histograms in a batched launch.
+struct ZeroJob {
+  const HistItem* items;
+  const int* count;
+  size_t words;  // 64-bit words per node histogram
+};
+
+// Device tables of histogram launches over many jobs (sb_train_many): job j
+// is described by Ls[j] (TILED layout; all FIXED or all FP32). Built once per
+// batch by hist_jobs_prepare and kept alive while its launches run. A launch
+// gives job j hist_grid[j] (zero_grid[j]) blocks, or none when the job builds
+// nothing at that step: the caller's offset tables say which.
+struct HistJobsPlan {
+  DBuf<char> devs;     // the jobs' launch descriptions
+  DBuf<ZeroJob> zero;  // [njobs]
+  std::vector<unsigned> hist_grid, zero_grid;
+  int njobs = 0;
+  int fixed = 0;
+  size_t smem = 0;
+};
+int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPlan* P);
+// Zeroes the jobs' current node histograms and builds them: one launch each.
+// d_xoff / d_zoff: [njobs + 1] block offsets of the two launches.
+int launch_hist_jobs(sb_ctx* ctx, const HistJobsPlan& P, const unsigned* d_xoff, unsigned hist_blocks,
+                     const unsigned* d_zoff, unsigned zero_blocks, int max_items);
+
 // One layout of the histogram's bin codes (HIST_LAYOUT_*; LANES: positions
 // per lane and tile, 1, 2 or 4).
 struct HistChoice {
@@ -233,6 +259,17 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L);
 int launch_zero_items(sb_ctx* ctx, const Ghist* g, const HistItem* items, const int* count,
                       int max_items);
 int hist_grid(sb_ctx* ctx, const Ghist* g, size_t rows_bound);
+// Depthwise boosters that can share batched round launches (no lossguide,
+// external gradients, timing, eval sets or row -> leaf output; TILED index).
+bool booster_batchable(const sb_booster* b);
+// `rounds` rounds of nb batchable boosters of one precision, on ctx's stream:
+// one launch per kernel step over all of them, recorded once as a graph.
+int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int rounds);
+// rounds[j] rounds of each of nb boosters: the batchable ones of the more
+// common precision with batched launches on ctx's stream, the others one
+// round at a time in turn on their own streams. status[j] gets each job's
+// result (entries not SB_OK on entry are skipped).
+int boosters_train_many(sb_ctx* ctx, sb_booster* const* bs, const int* rounds, int nb, int* status);
 
 // ----------------------------------------------------------------- model
 struct HostTree {

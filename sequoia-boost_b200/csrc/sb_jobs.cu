@@ -2,12 +2,13 @@
 // parameter sweeps) of uneven sizes trained together on one GPU.
 //
 // Each job gets its own binned matrix and device booster (train(), learner/
-// train.rs:107-113, per job), set up by a few host threads at once. Jobs are
-// spread round-robin over a pool of streams; the host then issues round r of every unfinished job before
-// round r + 1 of any, so the GPU always holds work of many jobs at once and
-// small jobs fill the SMs that one small job alone would leave idle. From its
-// third round on, a job's round is one CUDA-graph launch, so issuing a round
-// of every job costs the host a few microseconds per job.
+// train.rs:107-113, per job), set up by a few host threads at once, jobs
+// spread round-robin over a pool of streams. Depthwise jobs of one precision
+// then train as one batch: every round is one launch per kernel step for all
+// of them (their grids laid end to end, each block running its job's state),
+// recorded once as a CUDA graph and replayed. The jobs that cannot share
+// launches (lossguide, eval sets, the LANES layout, the other precision) are
+// issued round r of every job before round r + 1 of any over the pool.
 #include <algorithm>
 #include <thread>
 #include <vector>
@@ -58,12 +59,17 @@ int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams) {
     setup(0);
     for (std::thread& th : pool) th.join();
   }
-  // rounds, interleaved across jobs
-  int max_rounds = 0;
-  for (size_t j = 0; j < n_jobs; ++j) max_rounds = std::max(max_rounds, jobs[j].num_boost_round);
-  for (int r = 0; r < max_rounds && rc == SB_OK; ++r)
-    for (size_t j = 0; j < n_jobs; ++j)
-      if (jobs[j].status == SB_OK && r < jobs[j].num_boost_round) jobs[j].status = sb_booster_update(bo[j], 1);
+  // rounds: the jobs that can share launches run as one batch (one launch
+  // per kernel step for all of them), the others interleaved over the pool
+  if (rc == SB_OK && n_jobs > 0) {
+    std::vector<int> rounds(n_jobs), status(n_jobs);
+    for (size_t j = 0; j < n_jobs; ++j) {
+      rounds[j] = jobs[j].num_boost_round;
+      status[j] = jobs[j].status;
+    }
+    boosters_train_many(sctx[0], bo.data(), rounds.data(), (int)n_jobs, status.data());
+    for (size_t j = 0; j < n_jobs; ++j) jobs[j].status = status[j];
+  }
   // models
   for (size_t j = 0; j < n_jobs && rc == SB_OK; ++j)
     if (jobs[j].status == SB_OK) {
