@@ -336,10 +336,11 @@ typedef struct sb_job {
 /* No counterpart in the reference (it trains one job per call; cv() runs its
  * folds one after another). Trains independent jobs of any sizes together:
  * each gets its own binned matrix and device booster (set up by up to 8 host
- * threads), spread over n_streams streams (1..64). Depthwise jobs of one
- * precision train as one batch: each round is one launch per kernel step for
- * all of them. The others (lossguide, the LANES layout, the other precision)
- * are issued round r of every job before round r + 1 of any. Each model
+ * threads), spread over n_streams streams (1..64). Depthwise jobs train in
+ * batches of similar-size jobs of one precision (up to 8 batches at once, on
+ * their own streams): each round of a batch is one launch per kernel step
+ * for all its jobs. The others (lossguide, the LANES layout) are issued round
+ * r of every job before round r + 1 of any. Each model
  * equals the one sb_train would give for its job. Returns the first failing
  * job's status. */
 int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams);

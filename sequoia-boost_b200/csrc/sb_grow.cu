@@ -19,8 +19,11 @@
 //   -> k_round_end.
 // All frontier nodes of all K class trees are processed by each launch.
 #include <algorithm>
+#include <map>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <thread>
 
 #include "sb_internal.cuh"
 
@@ -2607,6 +2610,17 @@ bool booster_batchable(const sb_booster* b) {
          b->g->layout == HIST_LAYOUT_TILED;
 }
 
+// Before batched rounds: each job's own stream drained and its tree buffers
+// sized for `rounds` more rounds. Done before any batch records a graph: a
+// job's stream may be the stream another batch records on.
+int boosters_batch_prepare(sb_booster* b, int rounds) {
+  SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+  SB_TRY(booster_alloc_trees(b, (b->rounds_done + rounds) * b->K));
+  SB_TRY(booster_set_eval_smem(b));
+  SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+  return SB_OK;
+}
+
 int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int rounds) {
   if (nb <= 0 || rounds <= 0) return SB_OK;
   const int fixed = bs[0]->S.fixed;
@@ -2615,10 +2629,8 @@ int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int round
   for (int j = 0; j < nb; ++j) {
     sb_booster* b = bs[j];
     SB_REQUIRE(booster_batchable(b) && b->S.fixed == fixed, SB_ERR_INVALID_ARG, "internal: job %d not batchable", j);
-    SB_CUDA(cudaStreamSynchronize(b->ctx->stream));  // its set-up work
-    SB_TRY(booster_alloc_trees(b, (b->rounds_done + rounds) * b->K));
-    SB_TRY(booster_set_eval_smem(b));
-    SB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    SB_REQUIRE(b->tree_cap >= (b->rounds_done + rounds) * b->K, SB_ERR_INVALID_ARG,
+               "internal: job %d: tree buffers not prepared", j);
     maxD = std::max(maxD, b->D);
     maxK = std::max(maxK, b->K);
     esm = std::max(esm, eval_smem(b));
@@ -2791,18 +2803,38 @@ int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int round
   return rc;
 }
 
-int boosters_train_many(sb_ctx* ctx, sb_booster* const* bs, const int* rounds, int nb, int* status) {
-  // the batchable boosters of the more common precision train together
-  int nfix = 0, nflt = 0;
-  for (int j = 0; j < nb; ++j)
-    if (status[j] == SB_OK && bs[j] && rounds[j] > 0 && booster_batchable(bs[j])) (bs[j]->S.fixed ? nfix : nflt)++;
-  const int bfixed = nfix >= nflt ? 1 : 0;
-  std::vector<int> batch, rest;
+int boosters_train_many(sb_ctx* const* ctxs, int nctx, sb_booster* const* bs, const int* rounds, int nb,
+                        int* status) {
+  // batchable boosters train in groups that share one histogram kernel: the
+  // same precision and rows per warp instruction
+  // (SB_JOBS_BATCH=0: none, every job goes through the stream pool)
+  const char* eb = std::getenv("SB_JOBS_BATCH");
+  const bool batching = !(eb && std::strcmp(eb, "0") == 0);
+  std::map<std::pair<int, int>, std::vector<int>> groups;
+  std::vector<int> rest;
   for (int j = 0; j < nb; ++j) {
     if (status[j] != SB_OK || !bs[j] || rounds[j] <= 0) continue;
-    if (booster_batchable(bs[j]) && bs[j]->S.fixed == bfixed && nfix + nflt > 1) batch.push_back(j);
+    if (batching && booster_batchable(bs[j])) groups[{bs[j]->S.fixed, bs[j]->g->tiled_rl}].push_back(j);
     else rest.push_back(j);
   }
+  // a group becomes up to nctx batches of jobs of similar size (each batched
+  // launch waits for its largest job's part), one per stream, run by host
+  // threads at once so that the batches' launches overlap
+  std::vector<std::vector<int>> batches;
+  for (auto& kv : groups) {
+    std::vector<int>& v = kv.second;
+    if (v.size() < 2) {
+      rest.insert(rest.end(), v.begin(), v.end());
+      continue;
+    }
+    std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return bs[a]->n > bs[b]->n; });
+    const int parts = std::max(1, std::min(nctx, (int)v.size() / 2));
+    for (int q = 0; q < parts; ++q)
+      batches.emplace_back(v.begin() + (size_t)v.size() * q / parts, v.begin() + (size_t)v.size() * (q + 1) / parts);
+  }
+  for (const std::vector<int>& batch : batches)
+    for (int j : batch)
+      if (status[j] == SB_OK) status[j] = boosters_batch_prepare(bs[j], rounds[j]);
   // the others: round r of each before round r + 1 of any, on their own streams
   int max_rest = 0;
   for (int j : rest) max_rest = std::max(max_rest, rounds[j]);
@@ -2812,24 +2844,37 @@ int boosters_train_many(sb_ctx* ctx, sb_booster* const* bs, const int* rounds, i
         status[j] = booster_run(bs[j], 1);
         bs[j]->stats.rounds = bs[j]->rounds_done;
       }
-  // the batch, in segments of rounds that all its remaining jobs still have
-  int done = 0;
-  while (!batch.empty()) {
-    int seg = INT32_MAX;
-    for (int j : batch) seg = std::min(seg, rounds[j] - done);
-    std::vector<sb_booster*> part;
-    for (int j : batch) part.push_back(bs[j]);
-    const int rc = boosters_train_batched(ctx, part.data(), (int)part.size(), seg);
-    if (rc != SB_OK) {
-      for (int j : batch) status[j] = rc;
-      return rc;
+  // each batch in segments of rounds that all its remaining jobs still have
+  auto run_batch = [&](std::vector<int> batch, sb_ctx* ctx) {
+    cudaSetDevice(ctx->device);
+    batch.erase(std::remove_if(batch.begin(), batch.end(), [&](int j) { return status[j] != SB_OK; }), batch.end());
+    int done = 0;
+    while (!batch.empty()) {
+      int seg = INT32_MAX;
+      for (int j : batch) seg = std::min(seg, rounds[j] - done);
+      std::vector<sb_booster*> part;
+      for (int j : batch) part.push_back(bs[j]);
+      const int rc = boosters_train_batched(ctx, part.data(), (int)part.size(), seg);
+      if (rc != SB_OK) {
+        for (int j : batch) status[j] = rc;
+        return;
+      }
+      done += seg;
+      std::vector<int> next;
+      for (int j : batch)
+        if (rounds[j] > done) next.push_back(j);
+      batch.swap(next);
     }
-    done += seg;
-    std::vector<int> next;
-    for (int j : batch)
-      if (rounds[j] > done) next.push_back(j);
-    batch.swap(next);
+  };
+  for (size_t b0 = 0; b0 < batches.size(); b0 += (size_t)nctx) {
+    std::vector<std::thread> pool;
+    const size_t b1 = std::min(batches.size(), b0 + (size_t)nctx);
+    for (size_t b = b0 + 1; b < b1; ++b) pool.emplace_back(run_batch, batches[b], ctxs[b - b0]);
+    run_batch(batches[b0], ctxs[0]);
+    for (std::thread& th : pool) th.join();
   }
+  for (int j = 0; j < nb; ++j)
+    if (status[j] != SB_OK) return status[j];
   return SB_OK;
 }
 

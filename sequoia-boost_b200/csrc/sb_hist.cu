@@ -59,6 +59,7 @@ struct HistDev {
   unsigned long long* rows_done;  // sampled rows accumulated (or null)
   const uint32_t* pool_mask;      // [K][FW] features to accumulate (or null: all)
   int FW;
+  int rl;                         // TILED: log2 of the rows one warp instruction covers
 };
 
 __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
@@ -87,7 +88,9 @@ __device__ __forceinline__ void add_pair(unsigned a, unsigned hoff, uint32_t vg,
 // The shared partial is two planes of nent 32-bit words, g then h (FIXED:
 // int32 / uint32 integers; FP32: floats), so a warp's atomics spread over all
 // 32 banks. Every entry costs one add into each plane.
-template <bool FIXED>
+// RL >= 0: the rows per warp instruction (as log2) fixed at compile time;
+// RL < 0: read from the launch description (the batched kernel).
+template <bool FIXED, int RL>
 __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, unsigned gdx) {
   extern __shared__ unsigned long long sh_u64[];
   unsigned* sh_g = reinterpret_cast<unsigned*>(sh_u64);
@@ -122,11 +125,16 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     const unsigned sh_base = (unsigned)__cvta_generic_to_shared(sh_g), hoff = 4u * (unsigned)nent;
     const bool want_total = item.root && t == 0;
 
-    // lane `lane` owns the 4 consecutive features f0 + 4*lane .. +3 of the tile
-    // (only those of the tree's column pool); one 8-byte load per row fetches
-    // their 4 bins. Tiles start at multiples of 4 and rows are padded to a
-    // multiple of 8 bins, so the load is aligned and stays inside the row.
-    const int fl0 = 4 * lane;
+    // A warp instruction covers 2^rl rows: lane `lane` works on row slot
+    // lane >> (5 - rl) of it and owns the 4 consecutive features
+    // f0 + 4 * grp .. +3 of the tile, grp = its lane within the row's group
+    // (only features of the tree's column pool are added); one 8-byte load
+    // per row fetches their 4 bins. Tiles start at multiples of 4, hold at
+    // most 4 * 32 >> rl features, and rows are padded to a multiple of 8
+    // bins, so the load is aligned and stays inside the row.
+    const int rl = RL >= 0 ? RL : a.rl;
+    const int grp = lane & ((32 >> rl) - 1), rsub = lane >> (5 - rl);
+    const int fl0 = 4 * grp;
     const bool lane_on = fl0 < nf;
     bool fon[4];
 #pragma unroll
@@ -144,12 +152,13 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     }
     __syncthreads();
 
-    // Rows go through a warp in batches of TILED_ROWS, double-buffered: the
-    // codes and gradient pairs of the next batch are loaded before the adds of
-    // the current one, so the gather is in flight while the shared atomics
-    // issue. Lane q < TILED_ROWS holds row q of a batch (its id, loaded two
-    // batches ahead, and its gradient pair); the other lanes get them by
-    // shuffles. Every lane loads its 4 codes of each row.
+    // Rows go through a warp in batches of TILED_ROWS << rl, double-buffered:
+    // the codes and gradient pairs of the next batch are loaded before the
+    // adds of the current one, so the gather is in flight while the shared
+    // atomics issue. Lane i < the batch size holds row i of a batch (its id,
+    // loaded two batches ahead, and its gradient pair); the other lanes get
+    // them by shuffles. Step q of a batch covers its rows (q << rl) + slot,
+    // and every lane loads its 4 codes of its row.
     double tg = 0.0, th = 0.0;
     long long tqg = 0;
     unsigned long long tqh = 0;
@@ -157,7 +166,8 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     const size_t gcol = (size_t)item.k * a.n;
     const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
     constexpr int R = TILED_ROWS;
-    const uint32_t stride = (uint32_t)nwarps * R;
+    const uint32_t B = (uint32_t)R << rl;  // rows per batch (<= 32)
+    const uint32_t stride = (uint32_t)nwarps * B;
     // the gradient pair of the batch at p (lanes < its rows), counted into the totals
     auto load_grad = [&](uint32_t rid, uint32_t nr, uint32_t& g, uint32_t& h) {
       g = 0u;
@@ -188,37 +198,41 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     auto load_codes = [&](uint32_t rid, uint32_t nr, uint2 (&bv)[R]) {
 #pragma unroll
       for (int q = 0; q < R; ++q) {
-        const uint32_t id = __shfl_sync(0xFFFFFFFFu, rid, q);
-        bv[q] = ((uint32_t)q < nr && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + (size_t)id * a.Fp))
-                                              : make_uint2(0u, 0u);
+        const uint32_t src = ((uint32_t)q << rl) + (uint32_t)rsub;
+        const uint32_t id = __shfl_sync(0xFFFFFFFFu, rid, src);
+        bv[q] = (src < nr && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + (size_t)id * a.Fp))
+                                      : make_uint2(0u, 0u);
       }
     };
-    uint32_t p = pbeg + warp * R;
-    uint32_t rid_c = (lane < R && p + lane < pend) ? item.rows[p + lane] : 0u;
-    uint32_t nrow_c = p < pend ? min(pend - p, (uint32_t)R) : 0u;
+    uint32_t p = pbeg + warp * B;
+    uint32_t rid_c = ((uint32_t)lane < B && p + lane < pend) ? item.rows[p + lane] : 0u;
+    uint32_t nrow_c = p < pend ? min(pend - p, B) : 0u;
     uint32_t g_c, h_c;
     uint2 bv_c[R];
     load_grad(rid_c, nrow_c, g_c, h_c);
     load_codes(rid_c, nrow_c, bv_c);
-    uint32_t rid_n = (lane < R && p + stride + lane < pend) ? item.rows[p + stride + lane] : 0u;
+    uint32_t rid_n = ((uint32_t)lane < B && p + stride + lane < pend) ? item.rows[p + stride + lane] : 0u;
     for (; p < pend; p += stride) {
       const uint32_t pn = p + stride;
-      const uint32_t nrow_n = pn < pend ? min(pend - pn, (uint32_t)R) : 0u;
+      const uint32_t nrow_n = pn < pend ? min(pend - pn, B) : 0u;
       uint32_t g_n, h_n;
       uint2 bv_n[R];
       load_grad(rid_n, nrow_n, g_n, h_n);
       load_codes(rid_n, nrow_n, bv_n);
-      const uint32_t rid_nn = (lane < R && pn + stride + lane < pend) ? item.rows[pn + stride + lane] : 0u;
+      const uint32_t rid_nn =
+          ((uint32_t)lane < B && pn + stride + lane < pend) ? item.rows[pn + stride + lane] : 0u;
 #pragma unroll
       for (int q = 0; q < R; ++q) {
-        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, g_c, q);
-        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, h_c, q);
-        if ((uint32_t)q >= nrow_c) break;
+        const uint32_t src = ((uint32_t)q << rl) + (uint32_t)rsub;
+        const uint32_t vg = __shfl_sync(0xFFFFFFFFu, g_c, src);
+        const uint32_t vh = __shfl_sync(0xFFFFFFFFu, h_c, src);
+        if (((uint32_t)q << rl) >= nrow_c) break;  // no row of this step in any lane
+        const bool row_on = src < nrow_c;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const uint32_t w = j < 2 ? bv_c[q].x : bv_c[q].y;
           const unsigned idx = (j & 1) ? (w >> 16) : (w & 0xFFFFu);  // the tile-relative code
-          if (fon[j]) add_pair<FIXED>(sh_base + 4u * idx, hoff, vg, vh);
+          if (fon[j] && row_on) add_pair<FIXED>(sh_base + 4u * idx, hoff, vg, vh);
         }
       }
       g_c = g_n;
@@ -229,7 +243,7 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
       for (int q = 0; q < R; ++q) bv_c[q] = bv_n[q];
     }
     if (a.rows_done && t == 0 && nsampled) atomicAdd(a.rows_done, (unsigned long long)nsampled);
-    if (want_total && lane < ROWS_PER_WARP) {
+    if (want_total && (uint32_t)lane < B) {  // every lane that held rows of a batch
       if (FIXED) {
         atomicAdd(&s_tot_u[0], (unsigned long long)tqg);
         atomicAdd(&s_tot_u[1], tqh);
@@ -271,9 +285,9 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
   }
 }
 
-template <bool FIXED>
+template <bool FIXED, int RL>
 __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
-  hist_tiled_body<FIXED>(a, blockIdx.x, gridDim.x);
+  hist_tiled_body<FIXED, RL>(a, blockIdx.x, gridDim.x);
 }
 
 // Many indexes' histogram launches as one (sb_train_many): the x-blocks are
@@ -294,10 +308,30 @@ __device__ __forceinline__ int hist_job_of(const unsigned* xoff, int njobs, unsi
   return lo;
 }
 
-template <bool FIXED>
+template <bool FIXED, int RL>
 __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_jobs(HistJobs H) {
   const int j = hist_job_of(H.xoff, H.njobs, blockIdx.x);
-  hist_tiled_body<FIXED>(H.devs[j], blockIdx.x - H.xoff[j], H.xoff[j + 1] - H.xoff[j]);
+  hist_tiled_body<FIXED, RL>(H.devs[j], blockIdx.x - H.xoff[j], H.xoff[j + 1] - H.xoff[j]);
+}
+
+// The batched TILED kernel for a precision and rows per warp instruction.
+const void* tiled_jobs_kernel(bool fixed, int rl) {
+  switch (rl) {
+    case 1: return fixed ? (const void*)k_hist_jobs<true, 1> : (const void*)k_hist_jobs<false, 1>;
+    case 2: return fixed ? (const void*)k_hist_jobs<true, 2> : (const void*)k_hist_jobs<false, 2>;
+    case 3: return fixed ? (const void*)k_hist_jobs<true, 3> : (const void*)k_hist_jobs<false, 3>;
+    default: return fixed ? (const void*)k_hist_jobs<true, 0> : (const void*)k_hist_jobs<false, 0>;
+  }
+}
+
+// The TILED kernel for a precision and rows per warp instruction (log2).
+const void* tiled_kernel(bool fixed, int rl) {
+  switch (rl) {
+    case 1: return fixed ? (const void*)k_hist<true, 1> : (const void*)k_hist<false, 1>;
+    case 2: return fixed ? (const void*)k_hist<true, 2> : (const void*)k_hist<false, 2>;
+    case 3: return fixed ? (const void*)k_hist<true, 3> : (const void*)k_hist<false, 3>;
+    default: return fixed ? (const void*)k_hist<true, 0> : (const void*)k_hist<false, 0>;
+  }
 }
 
 // LANES layout (see sb_internal.cuh): lane l of every warp owns the features
@@ -528,13 +562,30 @@ namespace {
 // TILED layout: contiguous feature ranges whose bins and missing entries fit
 // the shared-memory budget, at most 128 features (4 per lane), starting at
 // multiples of 4 features.
+// Rows per warp instruction of the TILED kernel (as log2): a narrow matrix
+// leaves most of a warp's lanes without features when one row takes the
+// whole warp (4 features per lane), so up to 8 rows share an instruction:
+// at most 128 >> rl features per tile. SB_HIST_ROWS (1, 2, 4, 8) forces it.
+static int tiled_rows_log(size_t F) {
+  if (const char* e = std::getenv("SB_HIST_ROWS")) {
+    const int v = std::atoi(e);
+    if (v == 1) return 0;
+    if (v == 2) return 1;
+    if (v == 4) return 2;
+    if (v == 8) return 3;
+  }
+  return F <= 16 ? 3 : F <= 32 ? 2 : F <= 64 ? 1 : 0;
+}
+
 int plan_tiled(Ghist* g, size_t budget) {
   g->tiles.clear();
   const size_t F = g->F;
+  g->tiled_rl = tiled_rows_log(F);
+  const size_t max_tile = (size_t)MAX_TILE_FEATURES >> g->tiled_rl;
   size_t f0 = 0, maxb = 0;
   while (f0 < F) {
     size_t f1 = f0;
-    while (f1 < F && f1 - f0 < (size_t)MAX_TILE_FEATURES) {
+    while (f1 < F && f1 - f0 < max_tile) {
       size_t bins = g->h_foff[f1 + 1] - g->h_foff[f0];
       if ((bins + (f1 + 1 - f0)) * 8 > budget) break;
       f1++;
@@ -698,8 +749,8 @@ int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
     SB_CUDA(cudaStreamSynchronize(ctx->stream));
     g->hist_smem_bytes = lanes_smem(g);
   }
-  SB_TRY(raise_smem_limit((const void*)k_hist<false>, g->hist_smem_bytes));
-  SB_TRY(raise_smem_limit((const void*)k_hist<true>, g->hist_smem_bytes));
+  for (int fixed = 0; fixed < 2; ++fixed)
+    for (int rl = 0; rl < 4; ++rl) SB_TRY(raise_smem_limit(tiled_kernel(fixed != 0, rl), g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 1>, g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 1>, g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 2>, g->hist_smem_bytes));
@@ -757,7 +808,7 @@ const void* hist_kernel(const Ghist* g, bool fixed) {
       default: return fixed ? (const void*)k_hist_lanes<true, 4> : (const void*)k_hist_lanes<false, 4>;
     }
   }
-  return fixed ? (const void*)k_hist<true> : (const void*)k_hist<false>;
+  return tiled_kernel(fixed, g->tiled_rl);
 }
 
 }  // namespace
@@ -798,6 +849,7 @@ static HistDev hist_dev(const HistLaunch& L) {
   a.rows_done = L.rows_done;
   a.pool_mask = L.pool_mask;
   a.FW = (int)((L.g->F + 31) / 32);
+  a.rl = L.g->tiled_rl;
   return a;
 }
 
@@ -805,7 +857,7 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   const HistDev a = hist_dev(L);
   const int grid = hist_grid(ctx, L.g, L.rows_bound);
   const size_t sm = L.g->hist_smem_bytes;
-  void (*kern)(HistDev) = L.fixed ? k_hist<true> : k_hist<false>;
+  void (*kern)(HistDev) = reinterpret_cast<void (*)(HistDev)>(const_cast<void*>(tiled_kernel(L.fixed, L.g->tiled_rl)));
   if (L.g->layout == HIST_LAYOUT_LANES) {
     switch (L.g->slots) {
       case 1: kern = L.fixed ? k_hist_lanes<true, 1> : k_hist_lanes<false, 1>; break;
@@ -837,8 +889,9 @@ int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPl
   P->zero_grid.assign(nj, 0);
   for (int j = 0; j < nj; ++j) {
     const HistLaunch& L = Ls[j];
-    SB_REQUIRE(L.g->layout == HIST_LAYOUT_TILED && L.fixed == P->fixed, SB_ERR_INVALID_ARG,
-               "internal: batched histograms need the TILED layout and one precision");
+    SB_REQUIRE(L.g->layout == HIST_LAYOUT_TILED && L.fixed == P->fixed && L.g->tiled_rl == Ls[0].g->tiled_rl,
+               SB_ERR_INVALID_ARG,
+               "internal: batched histograms need the TILED layout, one precision and one row grouping");
     devs[j] = hist_dev(L);
     const size_t words = (L.g->total_bins + L.g->F) * 2;
     zero[j] = ZeroJob{L.items, L.count, words};
@@ -852,8 +905,8 @@ int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPl
   SB_TRY(P->zero.alloc(ctx, nj));
   SB_CUDA(cudaMemcpyAsync(P->devs.p, devs.data(), nj * sizeof(HistDev), cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(P->zero.p, zero.data(), nj * sizeof(ZeroJob), cudaMemcpyHostToDevice, st));
-  SB_TRY(raise_smem_limit((const void*)k_hist_jobs<true>, P->smem));
-  SB_TRY(raise_smem_limit((const void*)k_hist_jobs<false>, P->smem));
+  P->rl = Ls[0].g->tiled_rl;
+  SB_TRY(raise_smem_limit(tiled_jobs_kernel(P->fixed != 0, P->rl), P->smem));
   SB_CUDA(cudaStreamSynchronize(st));  // the host tables are released on return
   return SB_OK;
 }
@@ -866,8 +919,9 @@ int launch_hist_jobs(sb_ctx* ctx, const HistJobsPlan& P, const unsigned* d_xoff,
   H.devs = reinterpret_cast<const HistDev*>(P.devs.p);
   H.xoff = d_xoff;
   H.njobs = P.njobs;
-  if (P.fixed) SB_LAUNCH(ctx, k_hist_jobs<true>, hist_blocks, HIST_THREADS, P.smem, H);
-  else SB_LAUNCH(ctx, k_hist_jobs<false>, hist_blocks, HIST_THREADS, P.smem, H);
+  void (*kern)(HistJobs) =
+      reinterpret_cast<void (*)(HistJobs)>(const_cast<void*>(tiled_jobs_kernel(P.fixed != 0, P.rl)));
+  SB_LAUNCH(ctx, kern, hist_blocks, HIST_THREADS, P.smem, H);
   return SB_OK;
 }
 

@@ -146,6 +146,7 @@ struct Ghist {  // sb_ghist
   int has_categorical = 0;
   int layout = HIST_LAYOUT_TILED;  // HIST_LAYOUT_*
   int slots = 0;                   // LANES: code positions per lane and tile
+  int tiled_rl = 0;                // TILED: log2 of the rows one warp instruction covers
   // [n][Fp] bin codes of the histogram kernel: feature f of row r at
   // r * Fp + rpos[f], code = rbase[f] + local bin, or rmiss[f] for a missing
   // entry; unused positions hold 0xFFFF.
@@ -237,6 +238,7 @@ struct HistJobsPlan {
   std::vector<unsigned> hist_grid, zero_grid;
   int njobs = 0;
   int fixed = 0;
+  int rl = 0;  // rows per warp instruction (log2), the same for every job
   size_t smem = 0;
 };
 int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPlan* P);
@@ -265,11 +267,13 @@ bool booster_batchable(const sb_booster* b);
 // `rounds` rounds of nb batchable boosters of one precision, on ctx's stream:
 // one launch per kernel step over all of them, recorded once as a graph.
 int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int rounds);
-// rounds[j] rounds of each of nb boosters: the batchable ones of the more
-// common precision with batched launches on ctx's stream, the others one
-// round at a time in turn on their own streams. status[j] gets each job's
-// result (entries not SB_OK on entry are skipped).
-int boosters_train_many(sb_ctx* ctx, sb_booster* const* bs, const int* rounds, int nb, int* status);
+// rounds[j] rounds of each of nb boosters: the batchable ones in batches
+// (one launch per kernel step for a batch) of similar-size jobs, up to nctx
+// batches at once on the streams of ctxs; the others one round at a time in
+// turn on their own streams. status[j] gets each job's result (entries not
+// SB_OK on entry are skipped).
+int boosters_train_many(sb_ctx* const* ctxs, int nctx, sb_booster* const* bs, const int* rounds, int nb,
+                        int* status);
 
 // ----------------------------------------------------------------- model
 struct HostTree {

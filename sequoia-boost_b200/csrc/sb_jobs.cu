@@ -4,11 +4,13 @@
 // Each job gets its own binned matrix and device booster (train(), learner/
 // train.rs:107-113, per job), set up by a few host threads at once, jobs
 // spread round-robin over a pool of streams. Depthwise jobs of one precision
-// then train as one batch: every round is one launch per kernel step for all
-// of them (their grids laid end to end, each block running its job's state),
-// recorded once as a CUDA graph and replayed. The jobs that cannot share
-// launches (lossguide, eval sets, the LANES layout, the other precision) are
-// issued round r of every job before round r + 1 of any over the pool.
+// and one row grouping then train in batches: every round of a batch is one
+// launch per kernel step for all its jobs (their grids laid end to end, each
+// block running its job's state), recorded once as a CUDA graph and
+// replayed. Jobs are sorted by size into up to 8 batches of similar jobs that
+// run at once on their own streams. The jobs that cannot share launches
+// (lossguide, eval sets, the LANES layout) are issued round r of every job
+// before round r + 1 of any over the pool.
 #include <algorithm>
 #include <thread>
 #include <vector>
@@ -67,7 +69,7 @@ int sb_train_many(sb_ctx* ctx, sb_job* jobs, size_t n_jobs, int n_streams) {
       rounds[j] = jobs[j].num_boost_round;
       status[j] = jobs[j].status;
     }
-    boosters_train_many(sctx[0], bo.data(), rounds.data(), (int)n_jobs, status.data());
+    boosters_train_many(sctx.data(), std::min(S, 8), bo.data(), rounds.data(), (int)n_jobs, status.data());
     for (size_t j = 0; j < n_jobs; ++j) jobs[j].status = status[j];
   }
   // models

@@ -28,6 +28,24 @@ def hist_layout(name):
             os.environ["SB_HIST_LAYOUT"] = old
 
 
+@contextlib.contextmanager
+def hist_rows(rows):
+    """Indexes built inside the block give the TILED histogram kernel `rows`
+    rows (1, 2, 4 or 8) per warp instruction (None: by the feature count)."""
+    old = os.environ.get("SB_HIST_ROWS")
+    if rows is None:
+        os.environ.pop("SB_HIST_ROWS", None)
+    else:
+        os.environ["SB_HIST_ROWS"] = str(rows)
+    try:
+        yield
+    finally:
+        if old is None:
+            os.environ.pop("SB_HIST_ROWS", None)
+        else:
+            os.environ["SB_HIST_ROWS"] = old
+
+
 def mixed_data(n, f=12, seed=0, nan_frac=0.1, n_cat=0, card=8):
     """N(0,1), lognormal and Bernoulli columns, NaN holes, optional
     categorical columns at the end."""

@@ -172,3 +172,22 @@ def test_empty_row_draw_takes_one_row(sb, ctx, orc, grow_policy):
     ref = orc.train(x, y, p, 3)
     assert_trees_equal(m.export(), ref["model"].export())
     assert np.array_equal(m.predict_margin(sb.DMatrix(x)), ref["margins"].reshape(-1))
+
+
+def test_row_grouping_does_not_change_the_model(sb, ctx):
+    """Training on a narrow matrix with 1, 2, 4 or 8 rows per warp instruction
+    of the histogram kernel (fixed point) gives bit-identical models."""
+    from gpu_helpers import assert_trees_equal, hist_rows, mixed_data
+    x, _ = mixed_data(30_000, 13, seed=61)
+    y = (np.nan_to_num(x[:, 0]) - 0.5 * np.nan_to_num(x[:, 3]) > 0).astype(np.float32)
+    p = sb.TrainingParams(objective="binary:logistic", max_depth=6, eta=0.3, subsample=0.8,
+                          colsample_bytree=0.7, seed=5)
+    d = sb.DMatrix(x, labels=y)
+    models = []
+    for rows in (1, 2, 4, 8):
+        with hist_rows(rows):
+            models.append(sb.train(p, d, 6, ctx=ctx))
+    ref = models[0]
+    for m in models[1:]:
+        assert_trees_equal(m.export(), ref.export())
+        assert np.array_equal(m.predict_margin(d), ref.predict_margin(d))
