@@ -567,7 +567,8 @@ int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
   HistChoice choice;
   SB_TRY(hist_default_choice(ctx, g, &choice));
   const char* at = std::getenv("SB_HIST_AUTOTUNE");
-  const bool tune = !std::getenv("SB_HIST_LAYOUT") && !(at && std::strcmp(at, "0") == 0) && n >= TUNE_MIN_ROWS;
+  const bool tune = !std::getenv("SB_HIST_LAYOUT") && !std::getenv("SB_HIST_ROWS") &&
+                    !(at && std::strcmp(at, "0") == 0) && n >= TUNE_MIN_ROWS;
   const std::vector<HistChoice> cands = tune ? hist_candidates(ctx, g) : std::vector<HistChoice>();
   if (tune && cands.size() > 1) {
     int lg = 0;
@@ -600,7 +601,7 @@ int ghist_bin(sb_ctx* ctx, const float* d_X, Ghist* g) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tuned[key] = best;
       }
-      if (best.layout == last.layout && best.slots == last.slots) return SB_OK;  // built already
+      if (best.layout == last.layout && best.slots == last.slots && best.rl == last.rl) return SB_OK;  // built already
       choice = best;
     }
   }

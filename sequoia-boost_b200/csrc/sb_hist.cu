@@ -577,10 +577,10 @@ static int tiled_rows_log(size_t F) {
   return F <= 16 ? 3 : F <= 32 ? 2 : F <= 64 ? 1 : 0;
 }
 
-int plan_tiled(Ghist* g, size_t budget) {
+int plan_tiled(Ghist* g, size_t budget, int rl) {
   g->tiles.clear();
   const size_t F = g->F;
-  g->tiled_rl = tiled_rows_log(F);
+  g->tiled_rl = rl >= 0 ? rl : tiled_rows_log(F);
   const size_t max_tile = (size_t)MAX_TILE_FEATURES >> g->tiled_rl;
   size_t f0 = 0, maxb = 0;
   while (f0 < F) {
@@ -712,7 +712,7 @@ int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
   const size_t budget = smem_budget(ctx);
   const size_t F = g->F;
   if (c.layout == HIST_LAYOUT_TILED) {
-    SB_TRY(plan_tiled(g, budget));
+    SB_TRY(plan_tiled(g, budget, c.rl));
   } else {
     const int slots = c.slots;
     SB_REQUIRE(slots == 1 || slots == 2 || slots == 4, SB_ERR_INVALID_ARG, "internal: %d slots", slots);
@@ -781,14 +781,19 @@ int hist_default_choice(sb_ctx* ctx, Ghist* g, HistChoice* out) {
 }
 
 // The choices the autotuner times: TILED, and for up to 64 features (where
-// TILED keeps at most 16 of a warp's lanes busy) LANES with 1 and 2
-// positions per lane where the features pack. Wider matrices take TILED: on
+// one row per warp instruction keeps at most 16 of a warp's lanes busy)
+// TILED with 2, 4 or 8 rows per instruction and LANES with 1 and 2 positions
+// per lane where the features pack. Wider matrices take TILED: on
 // the 10M x 100 workload a whole round measured TILED faster at every level
 // (ncu: LANES cut the shared-atomic wavefronts by 2.4x but waited longer on
 // its 23 % longer rows), while a single timed launch ranked LANES first.
 std::vector<HistChoice> hist_candidates(sb_ctx* ctx, Ghist* g) {
-  std::vector<HistChoice> out{HistChoice{HIST_LAYOUT_TILED, 0}};
+  std::vector<HistChoice> out{HistChoice{HIST_LAYOUT_TILED, 0, 0}};
   if (g->F > 64) return out;
+  // TILED with 2, 4, 8 rows per warp instruction while a tile still holds
+  // every feature (128 >> rl features)
+  for (int rl = 1; rl <= 3 && (size_t)(MAX_TILE_FEATURES >> rl) >= g->F; ++rl)
+    out.push_back(HistChoice{HIST_LAYOUT_TILED, 0, rl});
   const std::vector<FeatureTile> keep = g->tiles;
   for (int slots : {1, 2}) {
     std::vector<std::vector<LanePlace>> places;

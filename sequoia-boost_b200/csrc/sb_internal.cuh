@@ -252,6 +252,7 @@ int launch_hist_jobs(sb_ctx* ctx, const HistJobsPlan& P, const unsigned* d_xoff,
 struct HistChoice {
   int layout;
   int slots;
+  int rl = -1;  // TILED: rows per warp instruction (log2); -1: by the feature count
 };
 int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c);
 int hist_default_choice(sb_ctx* ctx, Ghist* g, HistChoice* out);

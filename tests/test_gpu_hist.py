@@ -114,9 +114,10 @@ def test_local_bins_do_not_depend_on_layout(sb, ctx, layout):
 
 @pytest.mark.parametrize("f", [24, 60, 100])
 def test_autotuned_index_is_exact(sb, ctx, orc, f):
-    """Indexes of 200k rows and more time every layout that fits their shape
-    (TILED, LANES with 1, 2 or 4 positions per lane) on one histogram launch
-    and keep the fastest; whichever wins, the histograms are exact."""
+    """Indexes of 200k rows and more with at most 64 features time every
+    choice that fits their shape (TILED with 1, 2, 4 or 8 rows per warp
+    instruction, LANES with 1 or 2 positions per lane) and keep the fastest;
+    whichever wins, the histograms are exact."""
     n = 250_000
     x, _ = mixed_data(n, f, seed=f)
     g = random_gpair(n, seed=f + 1)
