@@ -1069,6 +1069,15 @@ __device__ __forceinline__ void k_eval_records_body(const BState& S, unsigned bx
   for (int j = lane; j < f; j += 32)
     if (in_mask(fm, j)) q = fmax(q, M[j]);
   q = warp_max(q);
+  // every record of this feature needs a gain above the running best, which
+  // starts at q: a feature whose best gain is not above q has none
+  if (!(M[f] > q)) {
+    if (lane == 0) {
+      rec->def_idx = -1;
+      rec->namb = 0;
+    }
+    return;
+  }
   const EvalNode E = eval_node(S, k, ni, d);
   CatScratch csv{};
   if (S.cat_cap > 0) csv = cat_scratch(ev_sm, warp, S.cat_bins);
