@@ -2666,6 +2666,7 @@ int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int round
     L.rows_done = nullptr;
     L.pool_mask = S.pool_mask;
     L.rows_bound = b->n * (size_t)b->K;
+    L.min_units = 2048;  // the batches' launches overlap: fewer, fuller CTAs for small nodes
   }
   HistJobsPlan hp;
   SB_TRY(hist_jobs_prepare(ctx, Ls, &hp));

@@ -60,6 +60,7 @@ struct HistDev {
   const uint32_t* pool_mask;      // [K][FW] features to accumulate (or null: all)
   int FW;
   int rl;                         // TILED: log2 of the rows one warp instruction covers
+  uint32_t min_units;             // fewest (row, tile) units per active CTA (0: all CTAs)
 };
 
 __device__ __forceinline__ int find_item(const uint64_t* prefix, int count, uint64_t pos) {
@@ -102,7 +103,14 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
   const uint64_t W = a.prefix[count];
   if (W == 0) return;
   const uint64_t U = W * (uint64_t)a.ntiles;
-  const uint64_t lo = U * bx / gdx, hi = U * (bx + 1) / gdx;
+  // with a.min_units set (batched jobs, whose launches overlap), a launch
+  // holding few rows uses fewer CTAs of at least that many (row, tile) units,
+  // so that zeroing and flushing a shared partial is paid for by enough rows;
+  // the other CTAs return. A lone launch spreads its rows over every CTA.
+  const uint64_t mu = a.min_units ? a.min_units : 1;
+  const uint64_t act = min((uint64_t)gdx, max((uint64_t)1, (U + mu - 1) / mu));
+  if (bx >= act) return;
+  const uint64_t lo = U * bx / act, hi = U * (bx + 1) / act;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 
   uint64_t u = lo;
@@ -855,6 +863,7 @@ static HistDev hist_dev(const HistLaunch& L) {
   a.pool_mask = L.pool_mask;
   a.FW = (int)((L.g->F + 31) / 32);
   a.rl = L.g->tiled_rl;
+  a.min_units = L.min_units;
   return a;
 }
 

@@ -218,6 +218,7 @@ struct HistLaunch {
   unsigned long long* rows_done;  // device counter of sampled rows, or null
   const uint32_t* pool_mask;      // device [K][ceil(F/32)]: features to accumulate, or null
   size_t rows_bound = 0;          // most rows one launch accumulates (0: unknown, full grid)
+  uint32_t min_units = 0;         // fewest (row, tile) units per active CTA (0: every CTA works)
 };
 
 // Zeroing of one job's node histograms in a batched launch.
