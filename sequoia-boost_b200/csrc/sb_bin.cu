@@ -372,6 +372,38 @@ __global__ void __launch_bounds__(1024) k_cuts_plan(
 // histogram codes go to row r at position rpos[f] (rbase[f] + local bin, or
 // rmiss[f] when missing); the feature-major copy holds the local bin itself,
 // MISSING_BIN when missing.
+// The local bin of value v of feature f: bin_of (quantile.rs:166-181), the
+// categorical form an exact match, MISSING_BIN for a missing value.
+__device__ __forceinline__ uint16_t local_bin(float v, int f, float missing, bool miss_nan,
+                                              const uint32_t* __restrict__ foff, const float* __restrict__ cuts,
+                                              const uint8_t* __restrict__ is_cat) {
+  if (is_missing_d(v, missing, miss_nan)) return MISSING_BIN;
+  const uint32_t s = foff[f], e = foff[f + 1];
+  const uint32_t len = e - s;
+  if (is_cat[f]) {
+    uint32_t lo = 0, hi = len, found = 0;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      const float c = cuts[s + mid];
+      if (c < v) lo = mid + 1;
+      else if (c > v) hi = mid;
+      else { found = mid; break; }
+    }
+    return (uint16_t)found;
+  }
+  uint32_t lo = 0, hi = len;  // partition_point(c <= v)
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
+  }
+  return (uint16_t)(lo < len - 1 ? lo : len - 1);
+}
+
+// A block bins a tile of BIN_TR rows x BIN_TF features: it reads the rows'
+// values in row order, writes the row-major codes row by row, and writes the
+// feature-major local bins column by column from a shared-memory copy of the
+// tile, so both layouts are stored with coalesced writes.
+constexpr int BIN_TR = 64, BIN_TF = 32;
 __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t n, int F, size_t Fp,
                                              float missing, const uint32_t* __restrict__ foff,
                                              const float* __restrict__ cuts,
@@ -381,38 +413,25 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
                                              const int* __restrict__ rmiss,
                                              uint16_t* __restrict__ bins,
                                              uint16_t* __restrict__ bins_col) {
+  __shared__ uint16_t tl[BIN_TF][BIN_TR + 2];  // local bins [feature][row]
   const bool miss_nan = isnan(missing);
-  const size_t total = n * (size_t)F;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const size_t r = i / F;
-    const int f = (int)(i - r * F);
-    const float v = X[i];
-    uint16_t local = MISSING_BIN;
-    if (!is_missing_d(v, missing, miss_nan)) {
-      const uint32_t s = foff[f], e = foff[f + 1];
-      const uint32_t len = e - s;
-      if (is_cat[f]) {
-        uint32_t lo = 0, hi = len, found = 0;
-        while (lo < hi) {
-          const uint32_t mid = (lo + hi) >> 1;
-          const float c = cuts[s + mid];
-          if (c < v) lo = mid + 1;
-          else if (c > v) hi = mid;
-          else { found = mid; break; }
-        }
-        local = (uint16_t)found;
-      } else {
-        uint32_t lo = 0, hi = len;  // partition_point(c <= v)
-        while (lo < hi) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
-        }
-        local = (uint16_t)(lo < len - 1 ? lo : len - 1);
-      }
+  const size_t r0 = (size_t)blockIdx.x * BIN_TR;
+  const int f0 = blockIdx.y * BIN_TF;
+  const int nr = (int)min((size_t)BIN_TR, n - r0), nf = min(BIN_TF, F - f0);
+  for (int i = threadIdx.x; i < BIN_TR * BIN_TF; i += blockDim.x) {
+    const int rr = i / BIN_TF, ff = i % BIN_TF;
+    if (rr < nr && ff < nf) {
+      const size_t r = r0 + rr;
+      const int f = f0 + ff;
+      const uint16_t local = local_bin(X[r * (size_t)F + f], f, missing, miss_nan, foff, cuts, is_cat);
+      tl[ff][rr] = local;
+      bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (uint16_t)rmiss[f] : (uint16_t)(rbase[f] + (int)local);
     }
-    bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (uint16_t)rmiss[f] : (uint16_t)(rbase[f] + (int)local);
-    bins_col[(size_t)f * n + r] = local;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < BIN_TR * BIN_TF; i += blockDim.x) {
+    const int ff = i / BIN_TR, rr = i % BIN_TR;
+    if (rr < nr && ff < nf) bins_col[(size_t)(f0 + ff) * n + r0 + rr] = tl[ff][rr];
   }
 }
 
@@ -633,9 +652,8 @@ int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_TRY(g->bins.alloc(ctx, n * g->Fp));
   SB_TRY(g->bins_col.alloc(ctx, n * F));
   SB_CUDA(cudaMemsetAsync(g->bins.p, 0xFF, g->bins.bytes(), st));  // unused positions: 0xFFFF
-  const size_t total = n * F;
-  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 32);
-  SB_LAUNCH(ctx, k_bin, blocks, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+  const dim3 bgrid((unsigned)((n + BIN_TR - 1) / BIN_TR), (unsigned)((F + BIN_TF - 1) / BIN_TF));
+  SB_LAUNCH(ctx, k_bin, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
             g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
   SB_CUDA(cudaStreamSynchronize(st));  // the host vectors are released on return
   return SB_OK;
