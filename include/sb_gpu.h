@@ -318,6 +318,20 @@ int sb_train(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
              const float* weights, const float* base_margin, const sb_train_params* p,
              int num_boost_round, sb_model** out);
 
+/* train() with booster = "dart" (learner/train.rs:384-456, model.rs:130-145):
+ * before each round the margins of the ensemble minus that round's dropout
+ * set (tree weights, dropped trees at 0) are predicted on the device and the
+ * round's K trees grow from their gradients; the new trees get weight
+ * 1 / (k + 1) and the k dropped trees are scaled by k / (k + 1), in f32. The
+ * dropout set is skipped with probability skip_drop, else each tree drops
+ * with probability rate_drop, at least one; its draws come from the
+ * SplitMix64 stream of sb_dart_key (include/sb_sampling.h), not rand 0.8.
+ * The returned model carries the tree weights. tree_method=hist only. */
+int sb_train_dart(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols,
+                  const uint8_t* feature_types, float missing, const float* labels,
+                  const float* weights, const float* base_margin, const sb_train_params* p,
+                  double rate_drop, double skip_drop, int num_boost_round, sb_model** out);
+
 /* One job of sb_train_many: the arguments of sb_train, plus its outputs. */
 typedef struct sb_job {
   const float* X;               /* [n_rows][n_cols], host */

@@ -202,6 +202,9 @@ SIGNATURES = {
     "sb_train_many": (I32, [P, ctypes.POINTER(SbJob), SZ, I32]),
     "sb_train": (I32, [P, F32P, SZ, SZ, U8P, ctypes.c_float, F32P, F32P, F32P,
                        ctypes.POINTER(SbTrainParams), I32, ctypes.POINTER(P)]),
+    "sb_train_dart": (I32, [P, F32P, SZ, SZ, U8P, ctypes.c_float, F32P, F32P, F32P,
+                            ctypes.POINTER(SbTrainParams), ctypes.c_double, ctypes.c_double, I32,
+                            ctypes.POINTER(P)]),
     "sb_model_create": (I32, [P, ctypes.POINTER(SbModelView), ctypes.POINTER(P)]),
     "sb_model_destroy": (I32, [P]),
     "sb_model_export_sizes": (I32, [P, I32P, I64P, I64P]),

@@ -759,48 +759,26 @@ def dart_dropout(seed, rnd, existing, rate_drop, skip_drop):
 
 
 def _train_dart(params, dtrain, num_boost_round, ctx):
-    """dart_round (learner/train.rs:384-456) over the device booster: per
-    round, the margins of the ensemble minus the dropout set are predicted on
-    the device (tree weights, dropped trees at 0) and handed to the booster,
-    whose next round grows the K new trees from their gradients; the new
+    """dart_round (learner/train.rs:384-456) through sb_train_dart: per round,
+    the margins of the ensemble minus the dropout set (dart_dropout's draws)
+    are predicted on the device with the tree weights and handed to the
+    booster, whose round grows the K new trees from their gradients; the new
     trees get weight 1/(k+1) and the k dropped trees are scaled by k/(k+1)."""
+    p, keep = params.to_c()
     k_out = params.num_class if params.objective.startswith("multi:") else 1
-    gh = GHistIndex(dtrain, max_bin=params.max_bin, ctx=ctx)
     bm = None
     if dtrain.base_margin is not None:
         bm = np.ascontiguousarray(np.broadcast_to(dtrain.base_margin.reshape(dtrain.n_rows, -1),
-                                                  (dtrain.n_rows, k_out)), np.float32)
-    b = Booster(gh, params, dtrain.labels, weights=dtrain.weights, base_margin=bm, ctx=ctx)
-    base0 = b.margins().copy()  # init_margin: base score or the dataset's base_margin
-    weights = np.zeros(0, np.float32)
-    arrays = None
-    info = None
-    for rnd in range(num_boost_round):
-        existing = len(weights)
-        dropped = dart_dropout(params.seed, rnd, existing, params.rate_drop, params.skip_drop)
-        if existing:
-            w = weights.copy()
-            w[dropped] = 0.0
-            m = BoostedModel.from_arrays(*arrays[:4], info[0], info[1], info[2], objective=params.objective,
-                                         weights=w, ctx=ctx)
-            d = DMatrix(dtrain.data, base_margin=None if bm is None else bm.reshape(-1), missing=dtrain.missing)
-            margins = m.predict_margin_limited(d, 0).reshape(dtrain.n_rows, k_out)
-        else:
-            margins = base0
-        b.set_margins(margins)
-        b.update(1)
-        kd = np.float32(len(dropped))
-        weights = np.concatenate([weights, np.full(k_out, np.float32(1.0) / (kd + np.float32(1.0)), np.float32)])
-        if dropped:
-            weights[dropped] = weights[dropped] * (kd / (kd + np.float32(1.0)))
-        grown = b.model()
-        arrays = grown.export()
-        info = grown.info()
-    grown = b.model()
-    off, nodes, coff, cats, _ = grown.export()
-    bs, k, f, _ = grown.info()
-    return BoostedModel.from_arrays(off, nodes, coff, cats, bs, k, f, objective=params.objective,
-                                    weights=weights, ctx=ctx)
+                                                  (dtrain.n_rows, k_out)), np.float32).reshape(-1)
+    ft = dtrain._ftypes()
+    h = ctypes.c_void_p()
+    A.check(A.lib().sb_train_dart(ctx.h, A.ptr(dtrain.data, ctypes.c_float), dtrain.n_rows, dtrain.n_cols,
+                                  A.ptr(ft, ctypes.c_uint8), dtrain.missing,
+                                  A.ptr(dtrain.labels, ctypes.c_float), A.ptr(dtrain.weights, ctypes.c_float),
+                                  A.ptr(bm, ctypes.c_float), ctypes.byref(p), float(params.rate_drop),
+                                  float(params.skip_drop), num_boost_round, ctypes.byref(h)))
+    del keep
+    return BoostedModel(h, ctx)
 
 
 class EarlyStopping:

@@ -2985,6 +2985,31 @@ int approx_train(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_
 
 }  // namespace sb
 
+namespace sb {
+
+// DART's dropout set of round `rnd` over the `existing` trees (train.rs:
+// 397-425): none with probability skip_drop, else each tree with probability
+// rate_drop, and at least one. Draws: a sequential stream from sb_dart_key,
+// each draw the SplitMix64 mix of the state before the state advances.
+std::vector<int> dart_dropout(uint64_t seed, uint64_t rnd, int existing, double rate_drop,
+                                     double skip_drop) {
+  uint64_t st = sb_dart_key(seed, rnd);
+  auto next = [&]() {
+    const uint64_t x = sb_mix64(st);
+    st += 0x9E3779B97F4A7C15ULL;
+    return x;
+  };
+  std::vector<int> dropped;
+  if (sb_u01(next()) < skip_drop || existing == 0) return dropped;
+  for (int i = 0; i < existing; ++i)
+    if (sb_u01(next()) < rate_drop) dropped.push_back(i);
+  if (dropped.empty())
+    dropped.push_back((int)(((unsigned __int128)next() * (unsigned __int128)existing) >> 64));
+  return dropped;
+}
+
+}  // namespace sb
+
 extern "C" {
 
 int sb_booster_create(sb_ctx* ctx, const sb_ghist* g, const sb_train_params* p, const float* labels,
@@ -3275,6 +3300,66 @@ int sb_train(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols, const ui
   sb_booster_destroy(b);
   sb_ghist_destroy(g);
   return s;
+}
+
+int sb_train_dart(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols, const uint8_t* feature_types,
+                  float missing, const float* labels, const float* weights, const float* base_margin,
+                  const sb_train_params* p, double rate_drop, double skip_drop, int num_boost_round,
+                  sb_model** out) {
+  using namespace sb;
+  SB_REQUIRE(ctx && X && labels && p && out, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_REQUIRE(num_boost_round >= 0, SB_ERR_INVALID_ARG, "negative num_boost_round");
+  SB_REQUIRE(rate_drop >= 0.0 && rate_drop <= 1.0, SB_ERR_INVALID_ARG,
+             "invalid parameter rate_drop=%g: must be in [0, 1]", rate_drop);
+  SB_REQUIRE(skip_drop >= 0.0 && skip_drop <= 1.0, SB_ERR_INVALID_ARG,
+             "invalid parameter skip_drop=%g: must be in [0, 1]", skip_drop);
+  SB_TRY(sb_train_params_validate(p));
+  SB_REQUIRE(p->tree_method != SB_TREE_APPROX, SB_ERR_UNSUPPORTED, "booster=dart trains tree_method=hist only");
+  SB_REQUIRE(n_rows > 0 && n_cols > 0, SB_ERR_INVALID_ARG, "empty dataset: zero rows or columns");
+  *out = nullptr;
+  SB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  // the rows stay on the device: every round predicts the ensemble on them
+  DBuf<float> dX;
+  SB_TRY(dX.alloc(ctx, n_rows * n_cols));
+  SB_CUDA(cudaMemcpyAsync(dX.p, X, dX.bytes(), cudaMemcpyHostToDevice, st));
+  sb_ghist* g = nullptr;
+  SB_TRY(sb_ghist_create_device(ctx, dX.p, n_rows, n_cols, feature_types, missing, p->max_bin, &g));
+  std::unique_ptr<sb_ghist, int (*)(sb_ghist*)> own_g(g, sb_ghist_destroy);
+  sb_booster* b = nullptr;
+  SB_TRY(sb_booster_create(ctx, g, p, labels, weights, base_margin, &b));
+  std::unique_ptr<sb_booster, int (*)(sb_booster*)> own_b(b, sb_booster_destroy);
+  const int K = b->K;
+  DBuf<float> dbm;
+  if (base_margin) {
+    SB_TRY(dbm.alloc(ctx, n_rows * K));
+    SB_CUDA(cudaMemcpyAsync(dbm.p, base_margin, dbm.bytes(), cudaMemcpyHostToDevice, st));
+  }
+  std::vector<float> w;  // tree weights (model.rs:130-145)
+  for (int rnd = 0; rnd < num_boost_round; ++rnd) {
+    const int existing = (int)w.size();
+    const std::vector<int> dropped = dart_dropout(p->seed, (uint64_t)rnd, existing, rate_drop, skip_drop);
+    if (existing) {  // margins of the ensemble with the dropped trees at weight 0
+      sb_model* m = nullptr;
+      SB_TRY(sb_booster_model(b, &m));
+      std::unique_ptr<sb_model, int (*)(sb_model*)> own_m(m, sb_model_destroy);
+      m->weights = w;
+      for (int t : dropped) m->weights[t] = 0.0f;
+      m->dev_valid = false;
+      SB_TRY(predict_margin_device(m, dX.p, n_rows, n_cols, missing, dbm.p, 1, 0, b->d_margin.p));
+      b->delta_pending = false;  // the booster grows the round's trees from these margins
+    }
+    SB_TRY(booster_run(b, 1));
+    b->stats.rounds = b->rounds_done;
+    const float kd = (float)dropped.size();
+    const float wn = 1.0f / (kd + 1.0f), ws = kd / (kd + 1.0f);
+    for (int c = 0; c < K; ++c) w.push_back(wn);
+    for (int t : dropped) w[t] = w[t] * ws;
+  }
+  SB_TRY(sb_booster_model(b, out));
+  (*out)->weights = w;
+  (*out)->dev_valid = false;
+  return SB_OK;
 }
 
 }  // extern "C"

@@ -353,6 +353,11 @@ int tree_depth(const HostTree& t);
 double node_mean_value(const HostTree& t, int id);  // learner/shap.rs:288-302
 // TreeSHAP (sb_shap.cu): the model's path data and tables, built once
 int shap_prepare(sb_model* m);
+// Margins of n device rows into d_out ([n][K]): base score, or the
+// per-row base margins d_base_margin ([n][K] when bm_kind == 1, [n] when 2),
+// plus the weighted leaf values of the first ntree_limit trees (0: all).
+int predict_margin_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing,
+                          const float* d_base_margin, int bm_kind, size_t ntree_limit, float* d_out);
 int predict_contribs_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing, float* d_out);
 int predict_interactions_device(sb_model* m, const float* d_X, size_t n, size_t F, float missing,
                                 float* d_out);
