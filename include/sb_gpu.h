@@ -191,6 +191,18 @@ int sb_ghist_cuts(const sb_ghist* g, uint32_t* feature_offset, float* cut_values
 /* Local bin of every entry, row-major n_rows * n_cols, 0xFFFF = missing. The
  * reference's global bin is feature_offset[f] + local (ghist.rs:48-82). */
 int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins);
+/* The device ELLPACK the histogram kernel reads, in the manner of
+ * GHistIndex::bins (ghist.rs:117), whose storage is tagged u16/u32: here
+ * u8 or u16 row-major codes, n_rows rows of `row_stride` codes.
+ * layout: 0 = TILED, 1 = LANES; code_bytes: 1 when the layout is TILED and
+ * every feature has at most 255 bins (then feature f's code sits at position
+ * f: its local bin, or its bin count when missing), else 2 (tile-relative
+ * histogram entries); rows_per_instruction: rows one warp instruction of the
+ * histogram kernel covers. Any pointer may be NULL. */
+int sb_ghist_layout(const sb_ghist* g, int* layout, int* code_bytes, size_t* row_stride,
+                    int* rows_per_instruction);
+/* Copies the n_rows * row_stride codes (code_bytes each) to `codes` (host). */
+int sb_ghist_codes(const sb_ghist* g, void* codes);
 
 /* HistCuts::from_dmatrix_weighted (data/quantile.rs:81-122, with
  * build_feature_cuts_weighted :253-316) + GHistIndex::from_dmatrix: the cuts

@@ -175,6 +175,9 @@ SIGNATURES = {
     "sb_ghist_create_device": (I32, [P, P, SZ, SZ, U8P, ctypes.c_float, I32, ctypes.POINTER(P)]),
     "sb_ghist_destroy": (I32, [P]),
     "sb_ghist_info": (I32, [P, ctypes.POINTER(SZ), ctypes.POINTER(SZ), ctypes.POINTER(SZ)]),
+    "sb_ghist_layout": (I32, [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(SZ),
+                              ctypes.POINTER(ctypes.c_int)]),
+    "sb_ghist_codes": (I32, [P, P]),
     "sb_ghist_cuts": (I32, [P, U32P, F32P, U8P]),
     "sb_ghist_bins": (I32, [P, U16P]),
     "sb_hist_build": (I32, [P, P, U32P, SZ, ctypes.POINTER(SbGradPair), SZ, I32, I32,

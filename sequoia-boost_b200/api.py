@@ -339,6 +339,25 @@ class GHistIndex(_Native):
     def total_bins(self):
         return self.info()[2]
 
+    def layout(self):
+        """The device ELLPACK's form: {"layout": "tiled"|"lanes", "code_bytes":
+        1|2, "row_stride": codes per row, "rows_per_instruction": 1..8}."""
+        lay, cb, rpi = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        st = ctypes.c_size_t()
+        A.check(A.lib().sb_ghist_layout(self.h, ctypes.byref(lay), ctypes.byref(cb), ctypes.byref(st),
+                                        ctypes.byref(rpi)))
+        return {"layout": "lanes" if lay.value == 1 else "tiled", "code_bytes": cb.value,
+                "row_stride": st.value, "rows_per_instruction": rpi.value}
+
+    def codes(self):
+        """The row-major histogram codes as stored on the device: [n][row_stride]
+        u8 or u16 (GHistIndex::bins, ghist.rs:117)."""
+        lay = self.layout()
+        n = self.info()[0]
+        out = np.zeros((n, lay["row_stride"]), np.uint8 if lay["code_bytes"] == 1 else np.uint16)
+        A.check(A.lib().sb_ghist_codes(self.h, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
     def cuts(self):
         """(feature_offset[F+1], cut_values[total_bins], is_categorical[F])."""
         n, f, t = self.info()

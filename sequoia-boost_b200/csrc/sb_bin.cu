@@ -404,6 +404,7 @@ __device__ __forceinline__ uint16_t local_bin(float v, int f, float missing, boo
 // feature-major local bins column by column from a shared-memory copy of the
 // tile, so both layouts are stored with coalesced writes.
 constexpr int BIN_TR = 64, BIN_TF = 32;
+template <typename Code>
 __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t n, int F, size_t Fp,
                                              float missing, const uint32_t* __restrict__ foff,
                                              const float* __restrict__ cuts,
@@ -411,7 +412,7 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
                                              const int* __restrict__ rpos,
                                              const int* __restrict__ rbase,
                                              const int* __restrict__ rmiss,
-                                             uint16_t* __restrict__ bins,
+                                             Code* __restrict__ bins,
                                              uint16_t* __restrict__ bins_col) {
   __shared__ uint16_t tl[BIN_TF][BIN_TR + 2];  // local bins [feature][row]
   const bool miss_nan = isnan(missing);
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
       const int f = f0 + ff;
       const uint16_t local = local_bin(X[r * (size_t)F + f], f, missing, miss_nan, foff, cuts, is_cat);
       tl[ff][rr] = local;
-      bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (uint16_t)rmiss[f] : (uint16_t)(rbase[f] + (int)local);
+      bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (Code)rmiss[f] : (Code)(rbase[f] + (int)local);
     }
   }
   __syncthreads();
@@ -649,12 +650,21 @@ int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_CUDA(cudaMemcpyAsync(rpos.p, g->h_rpos.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(rbase.p, g->h_rbase.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(rmiss.p, g->h_rmiss.data(), F * 4, cudaMemcpyHostToDevice, st));
-  SB_TRY(g->bins.alloc(ctx, n * g->Fp));
   SB_TRY(g->bins_col.alloc(ctx, n * F));
-  SB_CUDA(cudaMemsetAsync(g->bins.p, 0xFF, g->bins.bytes(), st));  // unused positions: 0xFFFF
   const dim3 bgrid((unsigned)((n + BIN_TR - 1) / BIN_TR), (unsigned)((F + BIN_TF - 1) / BIN_TF));
-  SB_LAUNCH(ctx, k_bin, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
-            g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
+  if (g->code_bytes == 1) {  // u8 codes: the u16 matrix is not kept
+    g->bins.release();
+    SB_TRY(g->bins8.alloc(ctx, n * g->Fp));
+    SB_CUDA(cudaMemsetAsync(g->bins8.p, 0xFF, g->bins8.bytes(), st));  // unused positions: 0xFF
+    SB_LAUNCH(ctx, k_bin<uint8_t>, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins8.p, g->bins_col.p);
+  } else {
+    g->bins8.release();
+    SB_TRY(g->bins.alloc(ctx, n * g->Fp));
+    SB_CUDA(cudaMemsetAsync(g->bins.p, 0xFF, g->bins.bytes(), st));  // unused positions: 0xFFFF
+    SB_LAUNCH(ctx, k_bin<uint16_t>, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
+  }
   SB_CUDA(cudaStreamSynchronize(st));  // the host vectors are released on return
   return SB_OK;
 }
@@ -722,6 +732,26 @@ int sb_ghist_bins(const sb_ghist* g, uint16_t* local_bins) {
   SB_CUDA(cudaStreamSynchronize(g->ctx->stream));
   for (size_t f = 0; f < g->F; ++f)
     for (size_t r = 0; r < g->n; ++r) local_bins[r * g->F + f] = col[f * g->n + r];
+  return SB_OK;
+}
+
+int sb_ghist_layout(const sb_ghist* g, int* layout, int* code_bytes, size_t* row_stride,
+                    int* rows_per_instruction) {
+  SB_REQUIRE(g != nullptr, SB_ERR_INVALID_ARG, "ghist is NULL");
+  if (layout) *layout = g->layout;
+  if (code_bytes) *code_bytes = g->code_bytes;
+  if (row_stride) *row_stride = g->Fp;
+  if (rows_per_instruction) *rows_per_instruction = g->layout == sb::HIST_LAYOUT_TILED ? 1 << g->tiled_rl : 1;
+  return SB_OK;
+}
+
+int sb_ghist_codes(const sb_ghist* g, void* codes) {
+  SB_REQUIRE(g && codes, SB_ERR_INVALID_ARG, "NULL argument");
+  SB_CUDA(cudaSetDevice(g->ctx->device));
+  const void* src = g->code_bytes == 1 ? (const void*)g->bins8.p : (const void*)g->bins.p;
+  SB_CUDA(cudaMemcpyAsync(codes, src, g->n * g->Fp * (size_t)g->code_bytes, cudaMemcpyDeviceToHost,
+                          g->ctx->stream));
+  SB_CUDA(cudaStreamSynchronize(g->ctx->stream));
   return SB_OK;
 }
 

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <memory>
 #include <thread>
+#include <tuple>
 
 #include "sb_internal.cuh"
 
@@ -81,7 +82,8 @@ struct BState {
   int* prev_count;          // [K] frontier nodes expanded by the last k_assign
   size_t n, Fp;
   // binned data
-  const uint16_t* bins;      // tile-relative codes, row-major
+  const uint16_t* bins;      // tile-relative codes, row-major (u16 codes)
+  const uint8_t* bins8;      // the same with u8 codes (bins null)
   const uint16_t* bins_col;  // the same, feature-major
   const int* fbase;          // code of local bin 0, per feature
   const int* fmiss;          // code of a missing entry, per feature
@@ -1760,14 +1762,15 @@ __global__ void k_lg_route(BState S) {
   const unsigned long long round = *S.round;
   const int K = S.K;
   for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < S.n; r += (size_t)gridDim.x * blockDim.x) {
-    const uint16_t* row = S.bins + r * S.Fp;
+    const uint16_t* row = S.bins ? S.bins + r * S.Fp : nullptr;
+    const uint8_t* row8 = S.bins8 ? S.bins8 + r * S.Fp : nullptr;
     for (int k = 0; k < K; ++k) {
       const sb_node* out = S.out_nodes + ((size_t)round * K + k) * S.maxn;
       int nid = 0;
       while (out[nid].left != -1) {
         const NodeSplit& sp = S.split[NI(S, k, nid)];
         const int f = sp.feature;
-        const int code = (int)row[S.rpos[f]];
+        const int code = row8 ? (int)row8[S.rpos[f]] : (int)row[S.rpos[f]];
         bool go;
         if (code == S.rmiss[f]) go = sp.default_left != 0;
         else {
@@ -2233,7 +2236,8 @@ int booster_init(sb_booster* b, sb_ctx* ctx, const sb_ghist* g, const sb_train_p
     if (g->h_is_cat[f]) S.cat_bins = std::max(S.cat_bins, (int)(g->h_foff[f + 1] - g->h_foff[f]));
   S.n = b->n;
   S.Fp = g->Fp;
-  S.bins = g->bins.p;
+  S.bins = g->code_bytes == 1 ? nullptr : g->bins.p;
+  S.bins8 = g->code_bytes == 1 ? g->bins8.p : nullptr;
   S.bins_col = g->bins_col.p;
   S.fbase = g->fbase.p;
   S.fmiss = g->fmiss.p;
@@ -2816,15 +2820,15 @@ int boosters_train_batched(sb_ctx* ctx, sb_booster* const* bs, int nb, int round
 int boosters_train_many(sb_ctx* const* ctxs, int nctx, sb_booster* const* bs, const int* rounds, int nb,
                         int* status) {
   // batchable boosters train in groups that share one histogram kernel: the
-  // same precision and rows per warp instruction
+  // same precision, rows per warp instruction and code width
   // (SB_JOBS_BATCH=0: none, every job goes through the stream pool)
   const char* eb = std::getenv("SB_JOBS_BATCH");
   const bool batching = !(eb && std::strcmp(eb, "0") == 0);
-  std::map<std::pair<int, int>, std::vector<int>> groups;
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
   std::vector<int> rest;
   for (int j = 0; j < nb; ++j) {
     if (status[j] != SB_OK || !bs[j] || rounds[j] <= 0) continue;
-    if (batching && booster_batchable(bs[j])) groups[{bs[j]->S.fixed, bs[j]->g->tiled_rl}].push_back(j);
+    if (batching && booster_batchable(bs[j])) groups[{bs[j]->S.fixed, bs[j]->g->tiled_rl, bs[j]->g->code_bytes}].push_back(j);
     else rest.push_back(j);
   }
   // a group becomes up to nctx batches of jobs of similar size (each batched

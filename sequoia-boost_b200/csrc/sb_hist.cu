@@ -42,10 +42,11 @@ constexpr int ROWS_PER_WARP = 8;        // LANES: rows per warp batch
 constexpr int TILED_ROWS = 4;           // TILED: rows per warp batch (two batches in flight)
 
 struct HistDev {
-  const uint16_t* bins;
+  const uint16_t* bins;  // u16 codes, or null with u8 codes in bins8
+  const uint8_t* bins8;
   const uint32_t* foff;
   size_t Fp;             // row stride of bins (u16)
-  const int* ent_gbin;   // LANES: (entry, lane) -> histogram bin, per tile
+  const int* ent_gbin;   // LANES: (entry, lane) -> histogram bin, per tile; u8 TILED: entry -> bin
   const int* slot_feat;  // LANES: feature of each code position of a row
   size_t n;              // gradient column stride
   int total_bins;
@@ -90,9 +91,17 @@ __device__ __forceinline__ void add_pair(unsigned a, unsigned hoff, uint32_t vg,
 // int32 / uint32 integers; FP32: floats), so a warp's atomics spread over all
 // 32 banks. Every entry costs one add into each plane.
 // RL >= 0: the rows per warp instruction (as log2) fixed at compile time;
-// RL < 0: read from the launch description (the batched kernel).
-template <bool FIXED, int RL>
+// RL < 0: read from the launch description.
+// U8: one-byte codes, the feature's local bin (its bin count when missing);
+// a feature's bins and its missing entry are contiguous in the partial, so an
+// entry's address is the feature's first entry plus the code, and the flush
+// maps entries to histogram bins through the tile's table (ent_gbin).
+template <bool U8> struct CodeWord { using T = uint2; };     // 4 u16 codes
+template <> struct CodeWord<true> { using T = uint32_t; };   // 4 u8 codes
+
+template <bool FIXED, int RL, bool U8>
 __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, unsigned gdx) {
+  using CW = typename CodeWord<U8>::T;
   extern __shared__ unsigned long long sh_u64[];
   unsigned* sh_g = reinterpret_cast<unsigned*>(sh_u64);
   __shared__ double s_tot_d[2];
@@ -145,11 +154,14 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     const int fl0 = 4 * grp;
     const bool lane_on = fl0 < nf;
     bool fon[4];
+    unsigned eb[4];  // U8: shared address of each owned feature's first entry
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int fl = fl0 + j;
       const int f = tile.f0 + fl;
       bool on = fl < nf;
+      eb[j] = sh_base;
+      if (U8 && on) eb[j] = sh_base + 4u * (a.foff[f] - (unsigned)tile.bin0 + (unsigned)fl);
       if (on && a.pool_mask && !((a.pool_mask[(size_t)item.k * a.FW + (f >> 5)] >> (f & 31)) & 1u)) on = false;
       fon[j] = on;
     }
@@ -172,7 +184,8 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     unsigned long long tqh = 0;
     unsigned int nsampled = 0;
     const size_t gcol = (size_t)item.k * a.n;
-    const uint16_t* bins_tile = a.bins + tile.f0 + fl0;
+    const uint16_t* bins_tile = U8 ? nullptr : a.bins + tile.f0 + fl0;
+    const uint8_t* bins8_tile = U8 ? a.bins8 + tile.f0 + fl0 : nullptr;
     constexpr int R = TILED_ROWS;
     const uint32_t B = (uint32_t)R << rl;  // rows per batch (<= 32)
     const uint32_t stride = (uint32_t)nwarps * B;
@@ -203,20 +216,23 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
       }
     };
     // the codes of the batch's rows (the lists hold sampled rows only)
-    auto load_codes = [&](uint32_t rid, uint32_t nr, uint2 (&bv)[R]) {
+    auto load_codes = [&](uint32_t rid, uint32_t nr, CW (&bv)[R]) {
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         const uint32_t src = ((uint32_t)q << rl) + (uint32_t)rsub;
         const uint32_t id = __shfl_sync(0xFFFFFFFFu, rid, src);
-        bv[q] = (src < nr && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + (size_t)id * a.Fp))
-                                      : make_uint2(0u, 0u);
+        if constexpr (U8)
+          bv[q] = (src < nr && lane_on) ? __ldg(reinterpret_cast<const uint32_t*>(bins8_tile + (size_t)id * a.Fp)) : 0u;
+        else
+          bv[q] = (src < nr && lane_on) ? __ldg(reinterpret_cast<const uint2*>(bins_tile + (size_t)id * a.Fp))
+                                        : make_uint2(0u, 0u);
       }
     };
     uint32_t p = pbeg + warp * B;
     uint32_t rid_c = ((uint32_t)lane < B && p + lane < pend) ? item.rows[p + lane] : 0u;
     uint32_t nrow_c = p < pend ? min(pend - p, B) : 0u;
     uint32_t g_c, h_c;
-    uint2 bv_c[R];
+    CW bv_c[R];
     load_grad(rid_c, nrow_c, g_c, h_c);
     load_codes(rid_c, nrow_c, bv_c);
     uint32_t rid_n = ((uint32_t)lane < B && p + stride + lane < pend) ? item.rows[p + stride + lane] : 0u;
@@ -224,7 +240,7 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
       const uint32_t pn = p + stride;
       const uint32_t nrow_n = pn < pend ? min(pend - pn, B) : 0u;
       uint32_t g_n, h_n;
-      uint2 bv_n[R];
+      CW bv_n[R];
       load_grad(rid_n, nrow_n, g_n, h_n);
       load_codes(rid_n, nrow_n, bv_n);
       const uint32_t rid_nn =
@@ -238,9 +254,14 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
         const bool row_on = src < nrow_c;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const uint32_t w = j < 2 ? bv_c[q].x : bv_c[q].y;
-          const unsigned idx = (j & 1) ? (w >> 16) : (w & 0xFFFFu);  // the tile-relative code
-          if (fon[j] && row_on) add_pair<FIXED>(sh_base + 4u * idx, hoff, vg, vh);
+          unsigned addr;
+          if constexpr (U8) {
+            addr = eb[j] + 4u * ((bv_c[q] >> (8 * j)) & 0xFFu);  // the feature's entry of the local bin
+          } else {
+            const uint32_t w = j < 2 ? bv_c[q].x : bv_c[q].y;
+            addr = sh_base + 4u * ((j & 1) ? (w >> 16) : (w & 0xFFFFu));  // the tile-relative code
+          }
+          if (fon[j] && row_on) add_pair<FIXED>(addr, hoff, vg, vh);
         }
       }
       g_c = g_n;
@@ -263,7 +284,8 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
     __syncthreads();
     // flush the partial into the node's HBM histogram
     for (int i = threadIdx.x; i < nent; i += blockDim.x) {
-      const int gi = i < tile.nbins ? tile.bin0 + i : a.total_bins + tile.f0 + (i - tile.nbins);
+      const int gi = U8 ? a.ent_gbin[tile.ent_off + i]
+                        : (i < tile.nbins ? tile.bin0 + i : a.total_bins + tile.f0 + (i - tile.nbins));
       if (FIXED) {
         const long long gq = (long long)(int)sh_g[i];
         const unsigned long long hq = sh_h[i];
@@ -293,9 +315,9 @@ __device__ __forceinline__ void hist_tiled_body(const HistDev& a, unsigned bx, u
   }
 }
 
-template <bool FIXED, int RL>
+template <bool FIXED, int RL, bool U8>
 __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(HistDev a) {
-  hist_tiled_body<FIXED, RL>(a, blockIdx.x, gridDim.x);
+  hist_tiled_body<FIXED, RL, U8>(a, blockIdx.x, gridDim.x);
 }
 
 // Many indexes' histogram launches as one (sb_train_many): the x-blocks are
@@ -316,30 +338,44 @@ __device__ __forceinline__ int hist_job_of(const unsigned* xoff, int njobs, unsi
   return lo;
 }
 
-template <bool FIXED, int RL>
+template <bool FIXED, int RL, bool U8>
 __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist_jobs(HistJobs H) {
   const int j = hist_job_of(H.xoff, H.njobs, blockIdx.x);
-  hist_tiled_body<FIXED, RL>(H.devs[j], blockIdx.x - H.xoff[j], H.xoff[j + 1] - H.xoff[j]);
+  hist_tiled_body<FIXED, RL, U8>(H.devs[j], blockIdx.x - H.xoff[j], H.xoff[j + 1] - H.xoff[j]);
 }
 
-// The batched TILED kernel for a precision and rows per warp instruction.
-const void* tiled_jobs_kernel(bool fixed, int rl) {
+template <bool FIXED, bool U8>
+const void* tiled_jobs_pick(int rl) {
   switch (rl) {
-    case 1: return fixed ? (const void*)k_hist_jobs<true, 1> : (const void*)k_hist_jobs<false, 1>;
-    case 2: return fixed ? (const void*)k_hist_jobs<true, 2> : (const void*)k_hist_jobs<false, 2>;
-    case 3: return fixed ? (const void*)k_hist_jobs<true, 3> : (const void*)k_hist_jobs<false, 3>;
-    default: return fixed ? (const void*)k_hist_jobs<true, 0> : (const void*)k_hist_jobs<false, 0>;
+    case 1: return (const void*)k_hist_jobs<FIXED, 1, U8>;
+    case 2: return (const void*)k_hist_jobs<FIXED, 2, U8>;
+    case 3: return (const void*)k_hist_jobs<FIXED, 3, U8>;
+    default: return (const void*)k_hist_jobs<FIXED, 0, U8>;
   }
 }
 
-// The TILED kernel for a precision and rows per warp instruction (log2).
-const void* tiled_kernel(bool fixed, int rl) {
+template <bool FIXED, bool U8>
+const void* tiled_pick(int rl) {
   switch (rl) {
-    case 1: return fixed ? (const void*)k_hist<true, 1> : (const void*)k_hist<false, 1>;
-    case 2: return fixed ? (const void*)k_hist<true, 2> : (const void*)k_hist<false, 2>;
-    case 3: return fixed ? (const void*)k_hist<true, 3> : (const void*)k_hist<false, 3>;
-    default: return fixed ? (const void*)k_hist<true, 0> : (const void*)k_hist<false, 0>;
+    case 1: return (const void*)k_hist<FIXED, 1, U8>;
+    case 2: return (const void*)k_hist<FIXED, 2, U8>;
+    case 3: return (const void*)k_hist<FIXED, 3, U8>;
+    default: return (const void*)k_hist<FIXED, 0, U8>;
   }
+}
+
+// The batched TILED kernel for a precision, rows per warp instruction (log2)
+// and code width.
+const void* tiled_jobs_kernel(bool fixed, int rl, bool u8) {
+  if (u8) return fixed ? tiled_jobs_pick<true, true>(rl) : tiled_jobs_pick<false, true>(rl);
+  return fixed ? tiled_jobs_pick<true, false>(rl) : tiled_jobs_pick<false, false>(rl);
+}
+
+// The TILED kernel for a precision, rows per warp instruction (log2) and
+// code width.
+const void* tiled_kernel(bool fixed, int rl, bool u8) {
+  if (u8) return fixed ? tiled_pick<true, true>(rl) : tiled_pick<false, true>(rl);
+  return fixed ? tiled_pick<true, false>(rl) : tiled_pick<false, false>(rl);
 }
 
 // LANES layout (see sb_internal.cuh): lane l of every warp owns the features
@@ -615,17 +651,49 @@ int plan_tiled(Ghist* g, size_t budget, int rl) {
   g->layout = HIST_LAYOUT_TILED;
   g->slots = 0;
   g->Fp = (F + 7) / 8 * 8;
+  // one-byte codes when every feature's local bins and its missing code fit
+  // (SB_HIST_CODES=2 keeps two bytes)
+  size_t max_nb = 0;
+  for (size_t f = 0; f < F; ++f) max_nb = std::max<size_t>(max_nb, g->h_foff[f + 1] - g->h_foff[f]);
+  const char* cb = std::getenv("SB_HIST_CODES");
+  g->code_bytes = (max_nb <= 255 && !(cb && std::atoi(cb) == 2)) ? 1 : 2;
   g->h_rpos.assign(F, 0);
   g->h_rbase.assign(F, 0);
   g->h_rmiss.assign(F, 0);
-  for (const FeatureTile& t : g->tiles)
+  int ent_off = 0;
+  for (FeatureTile& t : g->tiles) {
+    t.ent_off = ent_off;
+    ent_off += t.nbins + (t.f1 - t.f0);
     for (int f = t.f0; f < t.f1; ++f) {
       g->h_rpos[f] = f;
-      g->h_rbase[f] = (int)g->h_foff[f] - t.bin0;
-      g->h_rmiss[f] = t.nbins + (f - t.f0);
+      if (g->code_bytes == 1) {  // the local bin; the bin count when missing
+        g->h_rbase[f] = 0;
+        g->h_rmiss[f] = (int)(g->h_foff[f + 1] - g->h_foff[f]);
+      } else {  // the entry in the tile's partial: bins, then one missing entry per feature
+        g->h_rbase[f] = (int)g->h_foff[f] - t.bin0;
+        g->h_rmiss[f] = t.nbins + (f - t.f0);
+      }
     }
+  }
   g->hist_smem_bytes = maxb;
   return SB_OK;
+}
+
+// u8 TILED: the histogram bin of every shared entry, per tile: feature fl of
+// the tile owns entries foff[f] - bin0 + fl .. + its bin count (the last one
+// its missing entry, bin total_bins + f).
+std::vector<int> tiled_u8_entries(const Ghist* g) {
+  std::vector<int> eg;
+  for (const FeatureTile& t : g->tiles) {
+    eg.resize((size_t)t.ent_off + t.nbins + (t.f1 - t.f0), -1);
+    for (int f = t.f0; f < t.f1; ++f) {
+      const int nb = (int)(g->h_foff[f + 1] - g->h_foff[f]);
+      const size_t e0 = (size_t)t.ent_off + (g->h_foff[f] - t.bin0) + (f - t.f0);
+      for (int b = 0; b < nb; ++b) eg[e0 + b] = (int)g->h_foff[f] + b;
+      eg[e0 + nb] = (int)(g->total_bins + f);
+    }
+  }
+  return eg;
 }
 
 // One feature's place in the LANES layout.
@@ -721,6 +789,12 @@ int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
   const size_t F = g->F;
   if (c.layout == HIST_LAYOUT_TILED) {
     SB_TRY(plan_tiled(g, budget, c.rl));
+    if (g->code_bytes == 1) {
+      const std::vector<int> eg = tiled_u8_entries(g);
+      SB_TRY(g->ent_gbin.alloc(ctx, eg.size()));
+      SB_CUDA(cudaMemcpyAsync(g->ent_gbin.p, eg.data(), eg.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+      SB_CUDA(cudaStreamSynchronize(ctx->stream));  // the pageable copy must finish before eg goes away
+    }
   } else {
     const int slots = c.slots;
     SB_REQUIRE(slots == 1 || slots == 2 || slots == 4, SB_ERR_INVALID_ARG, "internal: %d slots", slots);
@@ -729,6 +803,7 @@ int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
                "a feature has too many bins for the lane layout");
     g->layout = HIST_LAYOUT_LANES;
     g->slots = slots;
+    g->code_bytes = 2;
     g->Fp = g->tiles.size() * 32 * slots;
     g->h_rpos.assign(F, 0);
     g->h_rbase.assign(F, 0);
@@ -758,7 +833,8 @@ int hist_prepare(sb_ctx* ctx, Ghist* g, HistChoice c) {
     g->hist_smem_bytes = lanes_smem(g);
   }
   for (int fixed = 0; fixed < 2; ++fixed)
-    for (int rl = 0; rl < 4; ++rl) SB_TRY(raise_smem_limit(tiled_kernel(fixed != 0, rl), g->hist_smem_bytes));
+    for (int rl = 0; rl < 4; ++rl)
+      for (int u8 = 0; u8 < 2; ++u8) SB_TRY(raise_smem_limit(tiled_kernel(fixed != 0, rl, u8 != 0), g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 1>, g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<true, 1>, g->hist_smem_bytes));
   SB_TRY(raise_smem_limit((const void*)k_hist_lanes<false, 2>, g->hist_smem_bytes));
@@ -821,7 +897,7 @@ const void* hist_kernel(const Ghist* g, bool fixed) {
       default: return fixed ? (const void*)k_hist_lanes<true, 4> : (const void*)k_hist_lanes<false, 4>;
     }
   }
-  return tiled_kernel(fixed, g->tiled_rl);
+  return tiled_kernel(fixed, g->tiled_rl, g->code_bytes == 1);
 }
 
 }  // namespace
@@ -845,7 +921,8 @@ int hist_grid(sb_ctx* ctx, const Ghist* g, size_t rows_bound) {
 // The kernel's description of one launch.
 static HistDev hist_dev(const HistLaunch& L) {
   HistDev a;
-  a.bins = L.g->bins.p;
+  a.bins = L.g->code_bytes == 1 ? nullptr : L.g->bins.p;
+  a.bins8 = L.g->code_bytes == 1 ? L.g->bins8.p : nullptr;
   a.foff = L.g->foff.p;
   a.Fp = L.g->Fp;
   a.ent_gbin = L.g->ent_gbin.p;
@@ -871,7 +948,8 @@ int launch_hist(sb_ctx* ctx, const HistLaunch& L) {
   const HistDev a = hist_dev(L);
   const int grid = hist_grid(ctx, L.g, L.rows_bound);
   const size_t sm = L.g->hist_smem_bytes;
-  void (*kern)(HistDev) = reinterpret_cast<void (*)(HistDev)>(const_cast<void*>(tiled_kernel(L.fixed, L.g->tiled_rl)));
+  void (*kern)(HistDev) = reinterpret_cast<void (*)(HistDev)>(
+      const_cast<void*>(tiled_kernel(L.fixed, L.g->tiled_rl, L.g->code_bytes == 1)));
   if (L.g->layout == HIST_LAYOUT_LANES) {
     switch (L.g->slots) {
       case 1: kern = L.fixed ? k_hist_lanes<true, 1> : k_hist_lanes<false, 1>; break;
@@ -903,9 +981,11 @@ int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPl
   P->zero_grid.assign(nj, 0);
   for (int j = 0; j < nj; ++j) {
     const HistLaunch& L = Ls[j];
-    SB_REQUIRE(L.g->layout == HIST_LAYOUT_TILED && L.fixed == P->fixed && L.g->tiled_rl == Ls[0].g->tiled_rl,
+    SB_REQUIRE(L.g->layout == HIST_LAYOUT_TILED && L.fixed == P->fixed && L.g->tiled_rl == Ls[0].g->tiled_rl &&
+                   L.g->code_bytes == Ls[0].g->code_bytes,
                SB_ERR_INVALID_ARG,
-               "internal: batched histograms need the TILED layout, one precision and one row grouping");
+               "internal: batched histograms need the TILED layout, one precision, one row grouping and one "
+               "code width");
     devs[j] = hist_dev(L);
     const size_t words = (L.g->total_bins + L.g->F) * 2;
     zero[j] = ZeroJob{L.items, L.count, words};
@@ -920,7 +1000,8 @@ int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPl
   SB_CUDA(cudaMemcpyAsync(P->devs.p, devs.data(), nj * sizeof(HistDev), cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(P->zero.p, zero.data(), nj * sizeof(ZeroJob), cudaMemcpyHostToDevice, st));
   P->rl = Ls[0].g->tiled_rl;
-  SB_TRY(raise_smem_limit(tiled_jobs_kernel(P->fixed != 0, P->rl), P->smem));
+  P->u8 = Ls[0].g->code_bytes == 1;
+  SB_TRY(raise_smem_limit(tiled_jobs_kernel(P->fixed != 0, P->rl, P->u8), P->smem));
   SB_CUDA(cudaStreamSynchronize(st));  // the host tables are released on return
   return SB_OK;
 }
@@ -934,7 +1015,7 @@ int launch_hist_jobs(sb_ctx* ctx, const HistJobsPlan& P, const unsigned* d_xoff,
   H.xoff = d_xoff;
   H.njobs = P.njobs;
   void (*kern)(HistJobs) =
-      reinterpret_cast<void (*)(HistJobs)>(const_cast<void*>(tiled_jobs_kernel(P.fixed != 0, P.rl)));
+      reinterpret_cast<void (*)(HistJobs)>(const_cast<void*>(tiled_jobs_kernel(P.fixed != 0, P.rl, P.u8)));
   SB_LAUNCH(ctx, kern, hist_blocks, HIST_THREADS, P.smem, H);
   return SB_OK;
 }

@@ -117,6 +117,9 @@ constexpr uint32_t UNSAMPLED = 0x80000000u;  // row-list flag: not in the subset
 //  TILED: row r holds feature f's code at position f (row stride Fp =
 //         round_up(F, 8)); the code is the entry's index in its feature tile's
 //         shared-memory partial, which holds the tile's bins in global order.
+//         With u8 codes (every feature at most 255 bins) the code is the
+//         feature's local bin, or its bin count when missing, and the partial
+//         holds each feature's bins followed by its missing entry.
 //  LANES: each tile gives each of the 32 lanes of a warp `slots` code
 //         positions (row stride Fp = tiles * 32 * slots); lane l owns the
 //         features placed in its slots, and the code is the entry's index e
@@ -131,14 +134,14 @@ struct FeatureTile {
   int bin0;       // foff[f0]
   int nbins;      // foff[f1] - foff[f0]
   int E;          // LANES: entries per lane (the partial has 32 * E words per plane)
-  int ent_off;    // LANES: offset of the tile's (entry, lane) -> histogram-bin table
+  int ent_off;    // LANES, u8 TILED: offset of the tile's entry -> histogram-bin table
   int slot_off;   // LANES: position of the tile's first code in a row
   int reserved;
 };
 
 struct Ghist {  // sb_ghist
   sb_ctx* ctx = nullptr;
-  size_t n = 0, F = 0, Fp = 0;   // Fp: row stride of `bins` in u16
+  size_t n = 0, F = 0, Fp = 0;   // Fp: row stride of the row-major codes, in codes
   size_t total_bins = 0;
   int max_bin = 0;
   float missing = NAN;
@@ -147,13 +150,20 @@ struct Ghist {  // sb_ghist
   int layout = HIST_LAYOUT_TILED;  // HIST_LAYOUT_*
   int slots = 0;                   // LANES: code positions per lane and tile
   int tiled_rl = 0;                // TILED: log2 of the rows one warp instruction covers
+  // Bytes per row-major code: 1 (u8) when the layout is TILED and every
+  // feature's bins and its missing entry fit a byte (at most 255 bins), else 2.
+  int code_bytes = 2;
   // [n][Fp] bin codes of the histogram kernel: feature f of row r at
   // r * Fp + rpos[f], code = rbase[f] + local bin, or rmiss[f] for a missing
-  // entry; unused positions hold 0xFFFF.
+  // entry; unused positions hold 0xFFFF (0xFF). `bins` holds u16 codes,
+  // `bins8` u8 codes (rbase 0, rmiss the feature's bin count); only the one
+  // of `code_bytes` is allocated.
   DBuf<uint16_t> bins;
+  DBuf<uint8_t> bins8;
   std::vector<int> h_rpos, h_rbase, h_rmiss;
   DBuf<int> rpos, rbase, rmiss;  // device copies of h_rpos, h_rbase, h_rmiss
-  DBuf<int> ent_gbin;      // LANES: per tile, [E][32] histogram bin of each (entry, lane), -1 unused
+  DBuf<int> ent_gbin;      // LANES: per tile, [E][32] histogram bin of each (entry, lane), -1 unused;
+                           // u8 TILED: per tile, the histogram bin of each shared entry
   DBuf<int> slot_feat;     // LANES: [Fp] feature of each code position, -1 unused
   // [F][n] local bins, feature-major, MISSING_BIN for a missing entry (the
   // partition reads them): code = fbase[f] + local, fmiss[f] when missing
@@ -240,6 +250,7 @@ struct HistJobsPlan {
   int njobs = 0;
   int fixed = 0;
   int rl = 0;  // rows per warp instruction (log2), the same for every job
+  bool u8 = false;  // one-byte codes, the same for every job
   size_t smem = 0;
 };
 int hist_jobs_prepare(sb_ctx* ctx, const std::vector<HistLaunch>& Ls, HistJobsPlan* P);
