@@ -54,14 +54,15 @@ __device__ __forceinline__ float key2f(uint32_t k) {
 
 constexpr int TILE_F = 32;
 constexpr int TILE_R = 128;
+constexpr int COUNT_THREADS = 256;
 
-// One streaming pass of the radix select over a (TILE_R rows x TILE_F
-// features) tile staged in shared memory; each warp walks one feature's
-// column so equal cells of consecutive rows aggregate before the atomic.
+// Levels 2 and 3 of the radix select: one streaming pass over a (TILE_R rows
+// x TILE_F features) tile staged in shared memory; each warp walks one
+// feature's column so equal cells of consecutive rows aggregate before the
+// atomic. Only values in the ranges the previous level refined are counted.
 template <int LEVEL>
-__global__ void __launch_bounds__(256) k_cuts_count(const float* __restrict__ X, size_t n, int F,
+__global__ void __launch_bounds__(COUNT_THREADS) k_cuts_count(const float* __restrict__ X, size_t n, int F,
                                                     float missing, int S,
-                                                    unsigned int* __restrict__ cnt1,
                                                     unsigned int* __restrict__ cnt2,
                                                     unsigned int* __restrict__ cnt3,
                                                     const short* __restrict__ map2,
@@ -73,52 +74,116 @@ __global__ void __launch_bounds__(256) k_cuts_count(const float* __restrict__ X,
   int f0 = blockIdx.y * TILE_F;
   int nf = min(TILE_F, F - f0);
   int nr = (int)min((size_t)TILE_R, n - r0);
-  for (int i = threadIdx.x; i < TILE_R * TILE_F; i += blockDim.x) {
-    int rr = i / TILE_F, ff = i % TILE_F;
-    float v = NAN;
-    if (rr < nr && ff < nf) v = X[(r0 + rr) * (size_t)F + f0 + ff];
-    tile[rr][ff] = v;
+  {  // every load of the thread's tile cells in flight together
+    constexpr int PER = TILE_R * TILE_F / COUNT_THREADS;
+    float v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int i = threadIdx.x + u * COUNT_THREADS;
+      const int rr = i / TILE_F, ff = i % TILE_F;
+      v[u] = (rr < nr && ff < nf) ? __ldg(X + (r0 + rr) * (size_t)F + f0 + ff) : NAN;
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int i = threadIdx.x + u * COUNT_THREADS;
+      tile[i / TILE_F][i % TILE_F] = v[u];
+    }
   }
   __syncthreads();
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int ff = warp; ff < nf; ff += nwarps) {
-    int f = f0 + ff;
-    if (LEVEL > 1 && plan[f].mode == MODE_DONE) continue;
-    for (int rb = 0; rb < nr; rb += 32) {
-      int rr = rb + lane;
-      unsigned int* addr = nullptr;
+  static_assert(LEVEL == 2 || LEVEL == 3, "level 1 counts in k_cuts_count1");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int STEPS = TILE_R / 32;
+  for (int ff = warp; ff < nf; ff += COUNT_THREADS / 32) {
+    const int f = f0 + ff;
+    if (plan[f].mode == MODE_DONE) continue;
+    // the counter of each of the lane's rows: the lookups of the steps are
+    // independent, so they are all issued before the first atomic
+    unsigned int* addr[STEPS];
+#pragma unroll
+    for (int q = 0; q < STEPS; ++q) {
+      const int rr = q * 32 + lane;
+      addr[q] = nullptr;
       if (rr < nr) {
-        float v = tile[rr][ff];
+        const float v = tile[rr][ff];
         bool miss = is_missing_d(v, missing, miss_nan);
         if (!miss && !miss_nan && isnan(v)) {
           plan[f].err = 1;
           miss = true;
         }
         if (!miss) {
-          uint32_t key = f2key(v);
-          uint32_t d1 = key >> 21;
-          if (LEVEL == 1) {
-            addr = cnt1 + (size_t)f * 2048 + d1;
-          } else {
-            int s2 = map2[(size_t)f * 2048 + d1];
-            if (s2 >= 0) {
-              uint32_t d2 = (key >> 10) & 0x7FFu;
-              if (LEVEL == 2) {
-                addr = cnt2 + ((size_t)f * S + s2) * 2048 + d2;
-              } else {
-                int s3 = map3[((size_t)f * S + s2) * 2048 + d2];
-                if (s3 >= 0) addr = cnt3 + ((size_t)f * S + s3) * 1024 + (key & 0x3FFu);
-              }
+          const uint32_t key = f2key(v);
+          const int s2 = map2[(size_t)f * 2048 + (key >> 21)];
+          if (s2 >= 0) {
+            const uint32_t d2 = (key >> 10) & 0x7FFu;
+            if (LEVEL == 2) {
+              addr[q] = cnt2 + ((size_t)f * S + s2) * 2048 + d2;
+            } else {
+              const int s3 = map3[((size_t)f * S + s2) * 2048 + d2];
+              if (s3 >= 0) addr[q] = cnt3 + ((size_t)f * S + s3) * 1024 + (key & 0x3FFu);
             }
           }
         }
       }
-      unsigned active = __ballot_sync(0xFFFFFFFFu, addr != nullptr);
-      if (addr) {
-        unsigned peers = __match_any_sync(active, (unsigned long long)addr);
-        if (lane == __ffs(peers) - 1) atomicAdd(addr, (unsigned)__popc(peers));
+    }
+#pragma unroll
+    for (int q = 0; q < STEPS; ++q) {
+      const unsigned active = __ballot_sync(0xFFFFFFFFu, addr[q] != nullptr);
+      if (addr[q]) {
+        const unsigned peers = __match_any_sync(active, (unsigned long long)addr[q]);
+        if (lane == __ffs(peers) - 1) atomicAdd(addr[q], (unsigned)__popc(peers));
       }
     }
+  }
+}
+
+// Level 1 of the radix select with shared-memory counters: a block takes
+// C1_FEATS consecutive features over a range of rows (4 lanes per row, one
+// feature each, so a warp reads 8 rows' 16-byte segments) and counts the top
+// 11 key bits of their present values in shared memory, then adds its
+// non-zero counters into cnt1. The counts are integers, so they equal those
+// of counting value by value in any order; values that would otherwise meet
+// in the few hot global counters of a feature's dense key range add in
+// shared memory.
+constexpr int C1_FEATS = 4;
+__global__ void __launch_bounds__(256) k_cuts_count1(const float* __restrict__ X, size_t n, int F, float missing,
+                                                     size_t rows_per_block, unsigned int* __restrict__ cnt1,
+                                                     FPlan* __restrict__ plan) {
+  __shared__ unsigned int s_c[C1_FEATS * 2048];
+  const bool miss_nan = isnan(missing);
+  const int f0 = blockIdx.y * C1_FEATS;
+  const int nf = min(C1_FEATS, F - f0);
+  const size_t r0 = (size_t)blockIdx.x * rows_per_block;
+  const size_t r1 = min(n, r0 + rows_per_block);
+  for (int i = threadIdx.x; i < C1_FEATS * 2048; i += blockDim.x) s_c[i] = 0u;
+  __syncthreads();
+  const int j = threadIdx.x % C1_FEATS;
+  const bool on = j < nf;
+  const size_t step = blockDim.x / C1_FEATS;
+  bool bad = false;  // NaN while the missing sentinel is not NaN
+  auto count = [&](float v) {
+    bool miss = is_missing_d(v, missing, miss_nan);
+    if (!miss && !miss_nan && isnan(v)) {
+      bad = true;
+      miss = true;
+    }
+    if (!miss) atomicAdd(&s_c[j * 2048 + (f2key(v) >> 21)], 1u);
+  };
+  size_t r = r0 + threadIdx.x / C1_FEATS;
+  if (on) {
+    for (; r + 3 * step < r1; r += 4 * step) {
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = __ldg(X + (r + u * step) * (size_t)F + f0 + j);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) count(v[u]);
+    }
+    for (; r < r1; r += step) count(__ldg(X + r * (size_t)F + f0 + j));
+  }
+  if (bad) plan[f0 + j].err = 1;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nf * 2048; i += blockDim.x) {
+    const unsigned c = s_c[i];
+    if (c) atomicAdd(&cnt1[(size_t)(f0 + i / 2048) * 2048 + (i % 2048)], c);
   }
 }
 
@@ -372,19 +437,16 @@ __global__ void __launch_bounds__(1024) k_cuts_plan(
 // histogram codes go to row r at position rpos[f] (rbase[f] + local bin, or
 // rmiss[f] when missing); the feature-major copy holds the local bin itself,
 // MISSING_BIN when missing.
-// The local bin of value v of feature f: bin_of (quantile.rs:166-181), the
-// categorical form an exact match, MISSING_BIN for a missing value.
-__device__ __forceinline__ uint16_t local_bin(float v, int f, float missing, bool miss_nan,
-                                              const uint32_t* __restrict__ foff, const float* __restrict__ cuts,
-                                              const uint8_t* __restrict__ is_cat) {
-  if (is_missing_d(v, missing, miss_nan)) return MISSING_BIN;
-  const uint32_t s = foff[f], e = foff[f + 1];
-  const uint32_t len = e - s;
-  if (is_cat[f]) {
+// The local bin of value v of a feature whose `len` cuts start at `cuts`:
+// bin_of (quantile.rs:166-181), the categorical form an exact match,
+// MISSING_BIN for a missing value.
+__device__ __forceinline__ uint16_t local_bin(float v, bool miss, const float* cuts, uint32_t len, bool cat) {
+  if (miss) return MISSING_BIN;
+  if (cat) {
     uint32_t lo = 0, hi = len, found = 0;
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
-      const float c = cuts[s + mid];
+      const float c = cuts[mid];
       if (c < v) lo = mid + 1;
       else if (c > v) hi = mid;
       else { found = mid; break; }
@@ -394,18 +456,21 @@ __device__ __forceinline__ uint16_t local_bin(float v, int f, float missing, boo
   uint32_t lo = 0, hi = len;  // partition_point(c <= v)
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    if (cuts[s + mid] <= v) lo = mid + 1; else hi = mid;
+    if (cuts[mid] <= v) lo = mid + 1; else hi = mid;
   }
   return (uint16_t)(lo < len - 1 ? lo : len - 1);
 }
 
-// A block bins a tile of BIN_TR rows x BIN_TF features: it reads the rows'
-// values in row order, writes the row-major codes row by row, and writes the
-// feature-major local bins column by column from a shared-memory copy of the
-// tile, so both layouts are stored with coalesced writes.
-constexpr int BIN_TR = 64, BIN_TF = 32;
+// A block bins BIN_TILES tiles of BIN_TR rows x BIN_TF features. It first
+// copies its features' cuts into shared memory (when they fit in
+// `sh_cut_cap` floats; else it searches them in global memory), so the
+// binary searches read shared memory. Per tile it reads the rows' values in
+// row order, writes the row-major codes row by row, and writes the
+// feature-major local bins column by column from a shared-memory copy of
+// the tile, so both layouts are stored with coalesced writes.
+constexpr int BIN_TR = 64, BIN_TF = 32, BIN_TILES = 16, BIN_THREADS = 256;
 template <typename Code>
-__global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t n, int F, size_t Fp,
+__global__ void __launch_bounds__(BIN_THREADS) k_bin(const float* __restrict__ X, size_t n, int F, size_t Fp,
                                              float missing, const uint32_t* __restrict__ foff,
                                              const float* __restrict__ cuts,
                                              const uint8_t* __restrict__ is_cat,
@@ -413,26 +478,61 @@ __global__ void __launch_bounds__(256) k_bin(const float* __restrict__ X, size_t
                                              const int* __restrict__ rbase,
                                              const int* __restrict__ rmiss,
                                              Code* __restrict__ bins,
-                                             uint16_t* __restrict__ bins_col) {
+                                             uint16_t* __restrict__ bins_col, int sh_cut_cap) {
+  extern __shared__ float s_cut[];
   __shared__ uint16_t tl[BIN_TF][BIN_TR + 2];  // local bins [feature][row]
+  __shared__ uint32_t s_off[BIN_TF + 1];
+  __shared__ int s_pos[BIN_TF], s_base[BIN_TF], s_miss[BIN_TF];
+  __shared__ uint8_t s_cat[BIN_TF];
   const bool miss_nan = isnan(missing);
-  const size_t r0 = (size_t)blockIdx.x * BIN_TR;
   const int f0 = blockIdx.y * BIN_TF;
-  const int nr = (int)min((size_t)BIN_TR, n - r0), nf = min(BIN_TF, F - f0);
-  for (int i = threadIdx.x; i < BIN_TR * BIN_TF; i += blockDim.x) {
-    const int rr = i / BIN_TF, ff = i % BIN_TF;
-    if (rr < nr && ff < nf) {
-      const size_t r = r0 + rr;
-      const int f = f0 + ff;
-      const uint16_t local = local_bin(X[r * (size_t)F + f], f, missing, miss_nan, foff, cuts, is_cat);
-      tl[ff][rr] = local;
-      bins[r * Fp + rpos[f]] = local == MISSING_BIN ? (Code)rmiss[f] : (Code)(rbase[f] + (int)local);
-    }
+  const int nf = min(BIN_TF, F - f0);
+  const uint32_t c0 = foff[f0], ncut = foff[f0 + nf] - c0;
+  const bool sh = ncut <= (uint32_t)sh_cut_cap;
+  for (int i = threadIdx.x; i <= nf; i += blockDim.x) s_off[i] = foff[f0 + i] - c0;
+  for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    s_pos[i] = rpos[f0 + i];
+    s_base[i] = rbase[f0 + i];
+    s_miss[i] = rmiss[f0 + i];
+    s_cat[i] = is_cat[f0 + i];
   }
+  if (sh)
+    for (uint32_t i = threadIdx.x; i < ncut; i += blockDim.x) s_cut[i] = cuts[c0 + i];
   __syncthreads();
-  for (int i = threadIdx.x; i < BIN_TR * BIN_TF; i += blockDim.x) {
-    const int ff = i / BIN_TR, rr = i % BIN_TR;
-    if (rr < nr && ff < nf) bins_col[(size_t)(f0 + ff) * n + r0 + rr] = tl[ff][rr];
+  const float* cb = sh ? s_cut : cuts + c0;
+  for (int t = 0; t < BIN_TILES; ++t) {
+    const size_t r0 = ((size_t)blockIdx.x * BIN_TILES + t) * BIN_TR;
+    if (r0 >= n) break;
+    const int nr = (int)min((size_t)BIN_TR, n - r0);
+    // all of a thread's values of the tile are loaded before the searches,
+    // so its loads are in flight together
+    constexpr int PER = BIN_TR * BIN_TF / BIN_THREADS;
+    float v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int i = threadIdx.x + u * BIN_THREADS;
+      const int rr = i / BIN_TF, ff = i % BIN_TF;
+      v[u] = (rr < nr && ff < nf) ? __ldg(X + (r0 + rr) * (size_t)F + f0 + ff) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int i = threadIdx.x + u * BIN_THREADS;
+      const int rr = i / BIN_TF, ff = i % BIN_TF;
+      if (rr < nr && ff < nf) {
+        const size_t r = r0 + rr;
+        const uint32_t s0 = s_off[ff];
+        const uint16_t local =
+            local_bin(v[u], is_missing_d(v[u], missing, miss_nan), cb + s0, s_off[ff + 1] - s0, s_cat[ff] != 0);
+        tl[ff][rr] = local;
+        bins[r * Fp + s_pos[ff]] = local == MISSING_BIN ? (Code)s_miss[ff] : (Code)(s_base[ff] + (int)local);
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BIN_TR * BIN_TF; i += blockDim.x) {
+      const int ff = i / BIN_TR, rr = i % BIN_TR;
+      if (rr < nr && ff < nf) bins_col[(size_t)(f0 + ff) * n + r0 + rr] = tl[ff][rr];
+    }
+    __syncthreads();
   }
 }
 
@@ -514,17 +614,24 @@ int ghist_build(sb_ctx* ctx, const float* d_X, size_t n, size_t F, const uint8_t
 
   dim3 cgrid((unsigned)((n + TILE_R - 1) / TILE_R), (unsigned)((F + TILE_F - 1) / TILE_F));
   SB_REQUIRE(cgrid.x <= 0x7FFFFFFFu, SB_ERR_UNSUPPORTED, "too many rows");
-  SB_LAUNCH(ctx, k_cuts_count<1>, cgrid, 256, 0, d_X, n, (int)F, missing, S, cnt1.p, cnt2.p, cnt3.p,
-            map2.p, map3.p, plan.p);
+  {  // level 1: shared counters; about 8 blocks per SM over all feature groups
+    const size_t groups = (F + C1_FEATS - 1) / C1_FEATS;
+    size_t nrb = std::max<size_t>(1, ((size_t)8 * ctx->num_sms + groups - 1) / groups);
+    nrb = std::min(nrb, (n + 1023) / 1024);
+    const size_t rpb = (n + nrb - 1) / nrb;
+    nrb = (n + rpb - 1) / rpb;
+    SB_LAUNCH(ctx, k_cuts_count1, dim3((unsigned)nrb, (unsigned)groups), 256, 0, d_X, n, (int)F, missing, rpb,
+              cnt1.p, plan.p);
+  }
   SB_LAUNCH(ctx, k_cuts_plan<1>, (unsigned)F, 1024, 0, (int)F, S, max_bin, g->is_cat.p, cnt1.p,
             cnt2.p, cnt3.p, map2.p, map3.p, slot_prefix.p, slot_base.p, trank.p, cut_tmp.p, ncut.p,
             plan.p);
-  SB_LAUNCH(ctx, k_cuts_count<2>, cgrid, 256, 0, d_X, n, (int)F, missing, S, cnt1.p, cnt2.p, cnt3.p,
+  SB_LAUNCH(ctx, k_cuts_count<2>, cgrid, COUNT_THREADS, 0, d_X, n, (int)F, missing, S, cnt2.p, cnt3.p,
             map2.p, map3.p, plan.p);
   SB_LAUNCH(ctx, k_cuts_plan<2>, (unsigned)F, 1024, 0, (int)F, S, max_bin, g->is_cat.p, cnt1.p,
             cnt2.p, cnt3.p, map2.p, map3.p, slot_prefix.p, slot_base.p, trank.p, cut_tmp.p, ncut.p,
             plan.p);
-  SB_LAUNCH(ctx, k_cuts_count<3>, cgrid, 256, 0, d_X, n, (int)F, missing, S, cnt1.p, cnt2.p, cnt3.p,
+  SB_LAUNCH(ctx, k_cuts_count<3>, cgrid, COUNT_THREADS, 0, d_X, n, (int)F, missing, S, cnt2.p, cnt3.p,
             map2.p, map3.p, plan.p);
   SB_LAUNCH(ctx, k_cuts_plan<3>, (unsigned)F, 1024, 0, (int)F, S, max_bin, g->is_cat.p, cnt1.p,
             cnt2.p, cnt3.p, map2.p, map3.p, slot_prefix.p, slot_base.p, trank.p, cut_tmp.p, ncut.p,
@@ -651,19 +758,29 @@ int bin_codes(sb_ctx* ctx, const float* d_X, Ghist* g) {
   SB_CUDA(cudaMemcpyAsync(rbase.p, g->h_rbase.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_CUDA(cudaMemcpyAsync(rmiss.p, g->h_rmiss.data(), F * 4, cudaMemcpyHostToDevice, st));
   SB_TRY(g->bins_col.alloc(ctx, n * F));
-  const dim3 bgrid((unsigned)((n + BIN_TR - 1) / BIN_TR), (unsigned)((F + BIN_TF - 1) / BIN_TF));
+  const size_t rows_per_block = (size_t)BIN_TR * BIN_TILES;
+  const dim3 bgrid((unsigned)((n + rows_per_block - 1) / rows_per_block), (unsigned)((F + BIN_TF - 1) / BIN_TF));
+  // the blocks' cuts go to shared memory up to the default 48 KB per block
+  // (less the static tile arrays); wider groups search them in global memory
+  const int sh_cap = (int)((48 * 1024 - 6 * 1024) / sizeof(float));
+  size_t sh_cuts = 0;
+  for (size_t f0 = 0; f0 < F; f0 += BIN_TF) {
+    const size_t c = g->h_foff[std::min(F, f0 + BIN_TF)] - g->h_foff[f0];
+    if (c <= (size_t)sh_cap) sh_cuts = std::max(sh_cuts, c);
+  }
+  const size_t bsm = sh_cuts * sizeof(float);
   if (g->code_bytes == 1) {  // u8 codes: the u16 matrix is not kept
     g->bins.release();
     SB_TRY(g->bins8.alloc(ctx, n * g->Fp));
     SB_CUDA(cudaMemsetAsync(g->bins8.p, 0xFF, g->bins8.bytes(), st));  // unused positions: 0xFF
-    SB_LAUNCH(ctx, k_bin<uint8_t>, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
-              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins8.p, g->bins_col.p);
+    SB_LAUNCH(ctx, k_bin<uint8_t>, bgrid, BIN_THREADS, bsm, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins8.p, g->bins_col.p, (int)sh_cuts);
   } else {
     g->bins8.release();
     SB_TRY(g->bins.alloc(ctx, n * g->Fp));
     SB_CUDA(cudaMemsetAsync(g->bins.p, 0xFF, g->bins.bytes(), st));  // unused positions: 0xFFFF
-    SB_LAUNCH(ctx, k_bin<uint16_t>, bgrid, 256, 0, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
-              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p);
+    SB_LAUNCH(ctx, k_bin<uint16_t>, bgrid, BIN_THREADS, bsm, d_X, n, (int)F, g->Fp, missing, g->foff.p, g->cuts.p,
+              g->is_cat.p, rpos.p, rbase.p, rmiss.p, g->bins.p, g->bins_col.p, (int)sh_cuts);
   }
   SB_CUDA(cudaStreamSynchronize(st));  // the host vectors are released on return
   return SB_OK;
