@@ -239,7 +239,9 @@ int sb_hist_subtract(sb_ctx* ctx, const sb_gradstats* parent, const sb_gradstats
  * bin per feature, so total_bins + n_cols must stay below about 524,000;
  * a larger index is rejected with SB_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress). The call copies small tables from host memory and
+ * waits for its result, so it cannot be recorded into a CUDA graph: while the
+ * context's stream is being captured it returns SB_ERR_UNSUPPORTED.
  * All calls on a device share the array, and the call clears the histogram
  * part itself: calls that overlap in time (from other threads, or other
  * contexts on the same device) race and must be serialised by the caller.

@@ -83,9 +83,15 @@ int sb_hist_build_static(sb_ctx* ctx, const sb_ghist* g, const uint32_t* d_rows,
              HB, need, (size_t)SB_STATIC_SCRATCH_BYTES);
 
   SB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  // the call copies its small tables from host memory and waits for its
+  // result, so it cannot be recorded into a graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  SB_CUDA(cudaStreamIsCapturing(st, &cap));
+  SB_REQUIRE(cap == cudaStreamCaptureStatusNone, SB_ERR_UNSUPPORTED,
+             "sb_hist_build_static cannot run while the context's stream is being captured");
   unsigned char* base = nullptr;
   SB_TRY(static_scratch(ctx->device, &base));
-  cudaStream_t st = ctx->stream;
   double2* hist = reinterpret_cast<double2*>(base);
   HistItem* d_item = reinterpret_cast<HistItem*>(base + off_item);
   uint64_t* d_prefix = reinterpret_cast<uint64_t*>(base + off_prefix);

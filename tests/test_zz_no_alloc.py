@@ -107,3 +107,53 @@ def test_static_scratch_through_a_second_context(sb, ctx, orc):
         got = d_out.cpu().numpy()
         assert np.all(np.abs(got - want) <= 1e-5 * mag + 1e-12)
         assert np.all(np.abs(got - ref) <= 1e-5 * mag + 1e-12)
+
+
+def test_static_scratch_from_a_second_context(sb, ctx, orc):
+    """A second context on the same device uses the array address that the
+    first context's call looked up (one lookup per device)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n, f = 20000, 12
+    x, _ = mixed_data(n, f, seed=23)
+    g = random_gpair(n, seed=7, logistic=True)
+    rows = np.arange(0, n, 2, dtype=np.uint32)
+    d_rows = torch.from_numpy(rows.astype(np.int32)).to(dev)
+    d_g = torch.from_numpy(np.ascontiguousarray(g, np.float32)).to(dev)
+    ref = orc.data(x).hist(rows, g)
+    mag = orc.data(x).hist(rows, np.abs(g))
+    ctx2 = sb.Context(0)
+    for c in (ctx, ctx2):
+        gh = sb.GHistIndex(sb.DMatrix(x), ctx=c)
+        total = gh.total_bins
+        d_out = torch.full((total, 2), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        rc = _static_build(sb, c, gh, d_rows.data_ptr(), rows.size, d_g.data_ptr(), n, d_out.data_ptr(), total)
+        assert rc == 0, sb._abi.lib().sb_last_error()
+        err = np.abs(d_out.cpu().numpy() - ref)
+        assert np.all(err <= 1e-5 * mag + 1e-12), float(np.max(err / (mag + 1e-30)))
+
+
+def test_static_scratch_refuses_a_capturing_stream(sb, ctx):
+    """While the context's stream records a CUDA graph the call returns
+    SB_ERR_UNSUPPORTED before it enqueues anything; the capture then ends with
+    an empty graph and the context stays usable."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n, f = 2000, 6
+    x, _ = mixed_data(n, f, seed=3)
+    gh = sb.GHistIndex(sb.DMatrix(x), ctx=ctx)
+    total = gh.total_bins
+    d_g = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    d_out = torch.zeros((total, 2), dtype=torch.float64, device=dev)
+    d_rows = torch.arange(n, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        rc = _static_build(sb, ctx, gh, d_rows.data_ptr(), n, d_g.data_ptr(), n, d_out.data_ptr(), total)
+    assert rc == sb._abi.SB_ERR_UNSUPPORTED
+    assert b"captured" in sb._abi.lib().sb_last_error()
+    del graph
+    rc = _static_build(sb, ctx, gh, d_rows.data_ptr(), n, d_g.data_ptr(), n, d_out.data_ptr(), total)
+    assert rc == 0, sb._abi.lib().sb_last_error()
