@@ -134,6 +134,7 @@ def test_static_scratch_from_a_second_context(sb, ctx, orc):
         assert np.all(err <= 1e-5 * mag + 1e-12), float(np.max(err / (mag + 1e-30)))
 
 
+@pytest.mark.filterwarnings("ignore:The CUDA Graph is empty")
 def test_static_scratch_refuses_a_capturing_stream(sb, ctx):
     """While the context's stream records a CUDA graph the call returns
     SB_ERR_UNSUPPORTED before it enqueues anything; the capture then ends with
