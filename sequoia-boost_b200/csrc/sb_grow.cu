@@ -2543,34 +2543,50 @@ int booster_set_eval_smem(sb_booster* b) {
   return SB_OK;
 }
 
-int booster_export(const sb_booster* b, sb_model* m) {
+// Appends to `m` the booster's trees it does not hold yet: m holds the
+// booster's first m->trees.size() trees (none, or what an earlier export or
+// append left), and only the trees after them cross to the host. New trees
+// get weight 1.
+int booster_export_append(const sb_booster* b, sb_model* m) {
   sb_ctx* ctx = b->ctx;
   const int ntrees = b->rounds_done * b->K;
-  std::vector<int> nn(ntrees), nc(ntrees);
-  std::vector<sb_node> nodes((size_t)ntrees * b->maxn);
-  std::vector<uint32_t> cats(b->S.cat_cap ? (size_t)ntrees * b->S.cat_cap : 0);
-  if (ntrees) {
-    SB_CUDA(cudaMemcpyAsync(nn.data(), b->d_out_nnodes.p, ntrees * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    SB_CUDA(cudaMemcpyAsync(nc.data(), b->d_out_ncats.p, ntrees * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    SB_CUDA(cudaMemcpyAsync(nodes.data(), b->d_out_nodes.p, nodes.size() * sizeof(sb_node),
+  const int t0 = (int)m->trees.size();
+  SB_REQUIRE(t0 <= ntrees, SB_ERR_INVALID_ARG, "internal: the model holds %d trees, the booster %d", t0, ntrees);
+  const int cnt = ntrees - t0;
+  const size_t cc = b->S.cat_cap;
+  std::vector<int> nn(cnt), nc(cnt);
+  std::vector<sb_node> nodes((size_t)cnt * b->maxn);
+  std::vector<uint32_t> cats(cc ? (size_t)cnt * cc : 0);
+  if (cnt) {
+    SB_CUDA(cudaMemcpyAsync(nn.data(), b->d_out_nnodes.p + t0, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(cudaMemcpyAsync(nc.data(), b->d_out_ncats.p + t0, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(cudaMemcpyAsync(nodes.data(), b->d_out_nodes.p + (size_t)t0 * b->maxn, nodes.size() * sizeof(sb_node),
                             cudaMemcpyDeviceToHost, ctx->stream));
     if (!cats.empty())
-      SB_CUDA(cudaMemcpyAsync(cats.data(), b->d_out_cats.p, cats.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      SB_CUDA(cudaMemcpyAsync(cats.data(), b->d_out_cats.p + (size_t)t0 * cc, cats.size() * 4,
+                              cudaMemcpyDeviceToHost, ctx->stream));
   }
   SB_CUDA(cudaStreamSynchronize(ctx->stream));
   m->trees.resize(ntrees);
-  m->weights.assign(ntrees, 1.0f);
-  for (int t = 0; t < ntrees; ++t) {
-    m->trees[t].nodes.assign(nodes.begin() + (size_t)t * b->maxn, nodes.begin() + (size_t)t * b->maxn + nn[t]);
+  m->weights.resize(ntrees, 1.0f);
+  for (int i = 0; i < cnt; ++i) {
+    const int t = t0 + i;
+    m->trees[t].nodes.assign(nodes.begin() + (size_t)i * b->maxn, nodes.begin() + (size_t)i * b->maxn + nn[i]);
     if (!cats.empty())
-      m->trees[t].cats.assign(cats.begin() + (size_t)t * b->S.cat_cap,
-                              cats.begin() + (size_t)t * b->S.cat_cap + nc[t]);
+      m->trees[t].cats.assign(cats.begin() + (size_t)i * cc, cats.begin() + (size_t)i * cc + nc[i]);
   }
   m->base_score = b->base_score;
   m->num_class = b->p.num_class;
   m->n_features = (int)b->g->F;
   m->objective = b->p.objective;
+  m->dev_valid = false;
   return SB_OK;
+}
+
+int booster_export(const sb_booster* b, sb_model* m) {
+  m->trees.clear();
+  m->weights.clear();
+  return booster_export_append(b, m);
 }
 
 int booster_trees(const sb_booster* b, BoosterTrees* v) {
@@ -3340,17 +3356,20 @@ int sb_train_dart(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols, con
     SB_CUDA(cudaMemcpyAsync(dbm.p, base_margin, dbm.bytes(), cudaMemcpyHostToDevice, st));
   }
   std::vector<float> w;  // tree weights (model.rs:130-145)
+  // one host ensemble for the whole loop: each round appends only the trees
+  // the previous round grew (the device copy is rebuilt for the prediction)
+  std::unique_ptr<sb_model, int (*)(sb_model*)> m(new sb_model, sb_model_destroy);
+  m->ctx = ctx;
+  SB_TRY(booster_export(b, m.get()));
   for (int rnd = 0; rnd < num_boost_round; ++rnd) {
     const int existing = (int)w.size();
     const std::vector<int> dropped = dart_dropout(p->seed, (uint64_t)rnd, existing, rate_drop, skip_drop);
     if (existing) {  // margins of the ensemble with the dropped trees at weight 0
-      sb_model* m = nullptr;
-      SB_TRY(sb_booster_model(b, &m));
-      std::unique_ptr<sb_model, int (*)(sb_model*)> own_m(m, sb_model_destroy);
+      SB_TRY(booster_export_append(b, m.get()));
       m->weights = w;
       for (int t : dropped) m->weights[t] = 0.0f;
       m->dev_valid = false;
-      SB_TRY(predict_margin_device(m, dX.p, n_rows, n_cols, missing, dbm.p, 1, 0, b->d_margin.p));
+      SB_TRY(predict_margin_device(m.get(), dX.p, n_rows, n_cols, missing, dbm.p, 1, 0, b->d_margin.p));
       b->delta_pending = false;  // the booster grows the round's trees from these margins
     }
     SB_TRY(booster_run(b, 1));
@@ -3360,9 +3379,10 @@ int sb_train_dart(sb_ctx* ctx, const float* X, size_t n_rows, size_t n_cols, con
     for (int c = 0; c < K; ++c) w.push_back(wn);
     for (int t : dropped) w[t] = w[t] * ws;
   }
-  SB_TRY(sb_booster_model(b, out));
-  (*out)->weights = w;
-  (*out)->dev_valid = false;
+  SB_TRY(booster_export_append(b, m.get()));
+  m->weights = w;
+  m->dev_valid = false;
+  *out = m.release();
   return SB_OK;
 }
 
